@@ -1,0 +1,292 @@
+"""goldbach-gpu_b200 -- Python binding over libgoldbach_b200.so (ctypes).
+
+The product is the sm_100a CUDA library behind include/gb/gb.h and the CLIs
+built on it (bin/goldbach, bin/single_check).  This module is the thin Python
+view of that C-ABI used by the tests and by bench.py.  There is no fallback:
+if the shared library is missing, importing the binding's `load()` raises.
+
+Loading by path (the directory name is not a Python identifier):
+    spec = importlib.util.spec_from_file_location(
+        "goldbach_gpu_b200", "<repo>/goldbach-gpu_b200/__init__.py")
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgoldbach_b200.so")
+BIN_DIR = os.path.join(HERE, "bin")
+
+GB_OK, GB_EINVAL, GB_ENOMEM, GB_ECUDA, GB_ETIMEOUT = 0, -1, -2, -3, -4
+GB_ECANCELED, GB_ENODEV, GB_EOVERFLOW, GB_EAGAIN = -5, -6, -7, -8
+GB_HIST_BINS = 4096
+GB_PHASE2_LIMIT_DEFAULT = 100_000_000
+GB_WINDOWS_PERSISTENT, GB_WINDOWS_PLAIN = 0, 1
+
+u64, u32, i32, vp = C.c_uint64, C.c_uint32, C.c_int, C.c_void_p
+
+
+class GbError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"gb status {status}: {msg}")
+        self.status = status
+
+
+class Config(C.Structure):
+    _fields_ = [("device_mem_budget", u64), ("max_n", u64), ("cand_limit", u64)]
+
+
+class RangeOpts(C.Structure):
+    _fields_ = [("seg_size", u64), ("p_small", u64), ("phase2_limit", u64),
+                ("chunk_evens", u32), ("halo", u32), ("shard_index", u32),
+                ("shard_count", u32), ("on_device", i32), ("stream", vp)]
+
+
+class RangeResult(C.Structure):
+    _fields_ = [("checked", u64), ("verified", u64), ("phase2_fallbacks", u64),
+                ("failures", u64), ("first_failure_n", u64), ("max_minp", u64),
+                ("num_segments", u64), ("queued", u64), ("kernel_launches", u64),
+                ("device_ms", C.c_double), ("kernel_ms", C.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class RangeOut(C.Structure):
+    _fields_ = [("verified_bits", vp), ("min_p", vp), ("minp_hist", vp),
+                ("seg_fallbacks", vp), ("seg_failures", vp), ("seg_hist", vp)]
+
+
+class SingleOpts(C.Structure):
+    _fields_ = [("p_limit", u64), ("on_device", i32), ("stream", vp)]
+
+
+class SingleResult(C.Structure):
+    _fields_ = [("found", u64), ("max_p", u64), ("kernel_launches", u64),
+                ("device_ms", C.c_double)]
+
+
+class Window(C.Structure):
+    _fields_ = [("start", u64), ("count", u64)]
+
+
+class WindowsOpts(C.Structure):
+    _fields_ = [("mode", i32), ("chunk_evens", u32), ("halo", u32),
+                ("phase2_limit", u64), ("on_device", i32), ("stream", vp)]
+
+
+class WindowResult(C.Structure):
+    _fields_ = [("verified", u64), ("failures", u64), ("max_minp", u64), ("minp_sum", u64)]
+
+
+class WindowsSummary(C.Structure):
+    _fields_ = [("total_n", u64), ("failures", u64), ("kernel_launches", u64),
+                ("device_ms", C.c_double)]
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Loads the CUDA library (raises FileNotFoundError / OSError if absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is not built: run `make -C goldbach-gpu_b200`")
+    L = C.CDLL(path)
+    P = C.POINTER
+    sig = {
+        "gb_device_count": (i32, []),
+        "gb_device_info": (i32, [i32, C.c_char_p, C.c_size_t, P(u64)]),
+        "gb_estimate_device_bytes": (u64, [P(Config)]),
+        "gb_create": (i32, [i32, P(Config), P(vp)]),
+        "gb_destroy": (None, [vp]),
+        "gb_strerror": (C.c_char_p, [i32]),
+        "gb_last_error": (C.c_char_p, [vp]),
+        "gb_mem_info": (i32, [vp, P(u64), P(u64)]),
+        "gb_num_segments": (u64, [u64, u64, u64]),
+        "gb_verify_range": (i32, [vp, u64, u64, P(RangeOpts), P(RangeResult), P(RangeOut)]),
+        "gb_sieve_bitset": (i32, [vp, u64, u64, vp, i32, vp]),
+        "gb_primes_upto": (i32, [vp, u64, vp, u64, P(u64)]),
+        "gb_is_prime_batch": (i32, [vp, vp, C.c_size_t, vp, i32, vp]),
+        "gb_check_single_batch": (i32, [vp, vp, C.c_size_t, vp, vp, P(SingleOpts), P(SingleResult)]),
+        "gb_verify_windows": (i32, [vp, P(Window), C.c_size_t, P(WindowsOpts), P(WindowResult),
+                                    vp, P(WindowsSummary)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name, None)
+        if f is None:  # entry point not in this build; calling it raises
+            continue
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):  # torch tensor
+        return a.data_ptr()
+    return int(a)
+
+
+def device_count() -> int:
+    return load().gb_device_count()
+
+
+@dataclass
+class RangeRun:
+    result: dict
+    min_p: np.ndarray | None = None
+    verified_bits: np.ndarray | None = None
+    hist: np.ndarray | None = None
+    seg_fallbacks: np.ndarray | None = None
+    seg_failures: np.ndarray | None = None
+    seg_hist: np.ndarray | None = None
+
+
+class Context:
+    """One gb_ctx: a CUDA device with its resident prime tables."""
+
+    def __init__(self, device: int = 0, budget: int = 0, max_n: int = 0, cand_limit: int = 0):
+        self.L = load()
+        self._h = vp()
+        cfg = Config(budget, max_n, cand_limit)
+        st = self.L.gb_create(device, C.byref(cfg), C.byref(self._h))
+        if st != GB_OK:
+            raise GbError(st, self.L.gb_strerror(st).decode())
+
+    def close(self):
+        if self._h:
+            self.L.gb_destroy(self._h)
+            self._h = vp()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st):
+        if st != GB_OK:
+            raise GbError(st, f"{self.L.gb_strerror(st).decode()}: "
+                              f"{self.L.gb_last_error(self._h).decode()}")
+
+    def mem_info(self):
+        held, budget = u64(), u64()
+        self._check(self.L.gb_mem_info(self._h, C.byref(held), C.byref(budget)))
+        return held.value, budget.value
+
+    # -- range -------------------------------------------------------------
+    def verify_range(self, start: int, limit: int, *, seg_size: int = 10_000_000,
+                     p_small: int = 1_000_000, phase2_limit: int = 0, chunk: int = 0,
+                     halo: int = 0, shard_index: int = 0, shard_count: int = 1,
+                     want_minp=False, want_bits=False, want_hist=True, want_seg=False,
+                     want_seg_hist=False, stream=None, device_out: dict | None = None,
+                     check: bool = True) -> RangeRun:
+        """Verifies every even n in [start, limit].  Host numpy outputs are
+        allocated on request; `device_out` maps RangeOut field names to device
+        pointers (torch tensors) and switches the call to on_device mode."""
+        L = self.L
+        lim = limit - (limit & 1)
+        st0 = max(4, start + (start & 1))
+        count = (lim - st0) // 2 + 1 if lim >= st0 else 0
+        nseg = L.gb_num_segments(start, limit, seg_size)
+        o = RangeOpts(seg_size, p_small, phase2_limit, chunk, halo, shard_index, shard_count,
+                      0, stream or None)
+        run = RangeRun(result={})
+        out = RangeOut()
+        if device_out is not None:
+            o.on_device = 1
+            for k, v in device_out.items():
+                setattr(out, k, _ptr(v))
+        else:
+            if want_minp:
+                run.min_p = np.zeros(count, np.uint32)
+                out.min_p = run.min_p.ctypes.data
+            if want_bits:
+                run.verified_bits = np.zeros((count + 31) // 32, np.uint32)
+                out.verified_bits = run.verified_bits.ctypes.data
+            if want_hist:
+                run.hist = np.zeros(GB_HIST_BINS, np.uint64)
+                out.minp_hist = run.hist.ctypes.data
+            if want_seg:
+                run.seg_fallbacks = np.zeros(nseg, np.uint32)
+                run.seg_failures = np.zeros(nseg, np.uint32)
+                out.seg_fallbacks = run.seg_fallbacks.ctypes.data
+                out.seg_failures = run.seg_failures.ctypes.data
+            if want_seg_hist:
+                run.seg_hist = np.zeros((nseg, GB_HIST_BINS), np.uint64)
+                out.seg_hist = run.seg_hist.ctypes.data
+        res = RangeResult()
+        st = L.gb_verify_range(self._h, start, limit, C.byref(o), C.byref(res), C.byref(out))
+        if check:
+            self._check(st)
+        run.result = res.as_dict()
+        run.result["status"] = st
+        return run
+
+    # -- tables / primality --------------------------------------------------
+    def sieve_bitset(self, q_lo: int, nbits: int) -> np.ndarray:
+        w = np.zeros((nbits + 31) // 32, np.uint32)
+        self._check(self.L.gb_sieve_bitset(self._h, q_lo, nbits, w.ctypes.data, 0, None))
+        return w
+
+    def primes_upto(self, limit: int) -> np.ndarray:
+        n = u64()
+        self._check(self.L.gb_primes_upto(self._h, limit, None, 0, C.byref(n)))
+        a = np.zeros(n.value, np.uint32)
+        self._check(self.L.gb_primes_upto(self._h, limit, a.ctypes.data, n.value, C.byref(n)))
+        return a
+
+    def is_prime(self, ns) -> np.ndarray:
+        ns = np.ascontiguousarray(ns, dtype=np.uint64)
+        out = np.zeros(len(ns), np.uint8)
+        self._check(self.L.gb_is_prime_batch(self._h, ns.ctypes.data, len(ns), out.ctypes.data,
+                                             0, None))
+        return out.astype(bool)
+
+    def check_single(self, ns, p_limit: int = 0, device_ptrs=None, stream=None):
+        """Minimal (p, q) for each even n.  device_ptrs=(n, p, q) runs on
+        device buffers (torch tensors) instead of host arrays."""
+        r = SingleResult()
+        if device_ptrs is not None:
+            n_t, p_t, q_t = device_ptrs
+            o = SingleOpts(p_limit, 1, stream or None)
+            self._check(self.L.gb_check_single_batch(self._h, _ptr(n_t), n_t.numel(), _ptr(p_t),
+                                                     _ptr(q_t), C.byref(o), C.byref(r)))
+            return None, None, r
+        ns = np.ascontiguousarray(ns, dtype=np.uint64)
+        p = np.zeros(len(ns), np.uint64)
+        q = np.zeros(len(ns), np.uint64)
+        o = SingleOpts(p_limit, 0, stream or None)
+        self._check(self.L.gb_check_single_batch(self._h, ns.ctypes.data, len(ns), p.ctypes.data,
+                                                 q.ctypes.data, C.byref(o), C.byref(r)))
+        return p, q, r
+
+    # -- windows -------------------------------------------------------------
+    def verify_windows(self, starts, counts, *, mode=GB_WINDOWS_PERSISTENT, chunk=0, halo=0,
+                       phase2_limit=0, want_minp=False, stream=None):
+        starts = np.asarray(starts, dtype=np.uint64)
+        counts = np.asarray(counts, dtype=np.uint64)
+        nw = len(starts)
+        w = (Window * nw)()
+        for i in range(nw):
+            w[i].start = int(starts[i])
+            w[i].count = int(counts[i])
+        res = (WindowResult * nw)()
+        minp = np.zeros(int(counts.sum()), np.uint32) if want_minp else None
+        s = WindowsSummary()
+        o = WindowsOpts(mode, chunk, halo, phase2_limit, 0, stream or None)
+        self._check(self.L.gb_verify_windows(self._h, w, nw, C.byref(o), res,
+                                             _ptr(minp), C.byref(s)))
+        per = [{f: getattr(res[i], f) for f, _ in WindowResult._fields_} for i in range(nw)]
+        return per, minp, {f: getattr(s, f) for f, _ in WindowsSummary._fields_}

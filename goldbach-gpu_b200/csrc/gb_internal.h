@@ -1,0 +1,149 @@
+// gb_internal.h -- argument blocks and launch functions shared by the host
+// side of the C-ABI (host/*.cpp) and the sm_100a kernels (kernels/*.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace gb {
+
+// Global counters of a call (device array of unsigned long long).
+enum Counter : int {
+  kCtrWork = 0,       // next work item (dynamic scheduling)
+  kCtrFallbacks = 1,  // n with minimal p > p_small (incl. failures)
+  kCtrFailures = 2,   // n without a partition within the bound
+  kCtrFirstFail = 3,  // smallest failing n (atomicMin; init ~0)
+  kCtrMaxP = 4,       // largest minimal p (atomicMax)
+  kCtrQueue = 5,      // entries pushed to the Phase-2 queue
+  kCtrQueueOvf = 6,   // set when the queue overflowed
+  kCtrWork2 = 7,      // second work counter (multi-stage pipelines)
+  kCtrCount = 8
+};
+
+// Phase-2 queue entry: an even n whose minimal p is beyond the window halo.
+struct QEntry {
+  uint64_t n;
+  uint64_t idx;   // output index (min_p / verified bits)
+  uint64_t unit;  // segment or window
+};
+
+// Everything the minimal-p search and the Phase-2 kernel read or account.
+struct SearchParams {
+  uint32_t halo;     // H: window holds q >= A - H + 1; primes p < H searched there
+  uint32_t nsearch;  // primes[1 .. nsearch) searched in the window (all p <= min(H-1, p_lim))
+  uint32_t klock;    // lockstep (word-parallel) phase covers k < klock
+  uint32_t kfb;      // first k whose prime exceeds p_small
+  uint64_t p_lim;    // candidate bound max(p_small, phase2_limit)
+  uint64_t p_small;
+  const uint32_t* primes;  // all primes ascending (2 first)
+  uint64_t nprimes;
+  unsigned long long* ctr;        // kCtrCount
+  unsigned long long* hist;       // nullable: GB_HIST_BINS
+  unsigned long long* unit_hist;  // nullable: units x GB_HIST_BINS
+  uint32_t* unit_fallbacks;       // nullable
+  uint32_t* unit_failures;        // nullable
+  unsigned long long* unit_maxp;  // nullable
+  unsigned long long* unit_psum;  // nullable: sum of minimal p per unit
+  uint32_t* minp;                 // nullable: per n
+  uint32_t* vbits;                // nullable: verified bits, prefilled with ones
+  QEntry* queue;
+  uint32_t queue_cap;
+};
+
+struct RangeArgs {
+  SearchParams s;
+  uint64_t start;          // first even n of the range
+  uint64_t total_count;    // even n in the range
+  uint64_t seg_size;       // even n per segment
+  uint32_t shard_index, shard_count;
+  uint64_t chunks_per_seg; // ceil(seg_size / chunk_evens)
+  uint64_t total_items;    // (segments of this shard) * chunks_per_seg
+  uint32_t chunk_evens;    // NE
+  uint32_t nbw;            // words of the q-window bitset (incl. padding)
+  const uint64_t* magic;   // Barrett reciprocals, magic[k] for primes[k]
+  uint32_t nsieve;         // primes[kWheelPrimeCount+1 .. nsieve) mark the window
+  uint32_t kcoop;          // ... those below kcoop warp-cooperatively
+  const uint32_t* wheel;   // wheel pattern table (kWheelWords)
+};
+
+struct SieveArgs {
+  uint64_t q_lo;           // odd
+  uint64_t nbits;
+  uint32_t tile_bits;      // bits per CTA tile (multiple of 32)
+  const uint32_t* primes;
+  const uint64_t* magic;
+  uint32_t nsieve;         // primes[1..nsieve) usable for marking
+  uint32_t kcoop;
+  const uint32_t* wheel;
+  uint32_t* out;           // ceil(nbits/32) words
+};
+
+// Batched windows: window w covers even n = start[w] + 2j, j < count[w]; its
+// q-bitset (odd q >= start - H + 1) has wbits[w] bits at word wbase[w].
+struct WinDesc {
+  uint64_t start;
+  uint64_t count;
+  uint64_t out_off;    // output index of its first n
+  uint64_t wbase;      // first word of its bitset in the global buffer
+  uint64_t wbits;      // bits of its bitset (H/2 + count + 64, rounded to 32)
+  uint64_t q_top;      // largest odd q of its bitset
+  uint32_t nsieve;     // primes[.. nsieve) needed by this window (p^2 <= q_top)
+  uint32_t orig;       // index of the window in the caller's order
+};
+
+struct WindowsArgs {
+  SearchParams s;
+  const WinDesc* win;      // nwin descriptors, sorted by q_top ascending
+  uint32_t nwin;
+  const uint64_t* tile_off;   // nwin+1 prefix sums of bitset tiles
+  const uint64_t* chunk_off;  // nwin+1 prefix sums of search chunks
+  uint64_t total_tiles, total_chunks;
+  uint32_t tile_bits;      // sieve tile (bits)
+  uint32_t chunk_evens;    // NE of the search
+  uint32_t nbw;            // shared words of a search window
+  uint32_t* bits;          // global window bitsets
+  const uint64_t* magic;
+  uint32_t nsmall;         // primes[.. nsmall) are marked in the tile sieve
+  uint32_t kcoop;
+  uint32_t nlarge;         // primes[nsmall .. nlarge) marked by the large-prime pass
+  const uint32_t* wheel;
+};
+
+// kernels/tables.cu
+cudaError_t launch_wheel_init(uint32_t* wheel, cudaStream_t s);
+cudaError_t launch_sieve_bits(const SieveArgs& a, cudaStream_t s);
+// Appends the primes of `bits` (odd-only from q_lo) after `prefix` entries of
+// `primes`; writes the new total into *d_total (device) and magic[] for them.
+cudaError_t launch_compact_primes(const uint32_t* bits, uint64_t nbits, uint64_t q_lo,
+                                  uint32_t* primes, uint64_t* magic, uint64_t prefix,
+                                  uint64_t cap, unsigned long long* d_total,
+                                  uint32_t* scratch_blocks, uint32_t nblocks_cap,
+                                  cudaStream_t s);
+size_t compact_scratch_blocks(uint64_t nbits);
+
+// kernels/range.cu
+size_t range_smem_bytes(const RangeArgs& a);
+int range_max_blocks_per_sm(const RangeArgs& a);
+cudaError_t launch_range(const RangeArgs& a, int grid, cudaStream_t s);
+cudaError_t launch_fallback(const SearchParams& s, int grid, cudaStream_t st);
+
+// kernels/windows.cu: the three stages for all windows (w_only = ~0u) or for
+// one window; grids are chosen by the caller.
+cudaError_t launch_window_stages(const WindowsArgs& a, uint32_t w_only, int grid_tile,
+                                 int grid_large, int grid_search, cudaStream_t s, int* launches);
+
+// kernels/single.cu
+struct SingleArgs {
+  const uint64_t* n;
+  uint64_t count;
+  uint64_t* p_out;
+  uint64_t* q_out;
+  const uint32_t* primes;
+  uint64_t nprimes;
+  uint64_t p_lim;
+  unsigned long long* ctr;  // [0] work, [1] found, [2] max p
+};
+cudaError_t launch_single(const SingleArgs& a, int grid, cudaStream_t s);
+cudaError_t launch_is_prime(const uint64_t* n, uint64_t count, uint8_t* out, cudaStream_t s);
+
+}  // namespace gb

@@ -1,0 +1,234 @@
+/*
+ * gb.h -- C-ABI of the B200 Goldbach verifier (libgoldbach_b200.so).
+ *
+ * The reference project (isaac-6/goldbach-gpu) exposes no library: its
+ * boundary is the `goldbach` and `single_check` processes, and the seam below
+ * them is run_gpu_worker() in src/goldbach.cu:378-500.  This header is the
+ * library boundary those CLIs are rebuilt on; each entry point names the
+ * reference code it replaces.
+ *
+ * Conventions
+ *   - Plain C types only.  Every entry point returns a gb_status (0 = ok,
+ *     negative = error); no C++ exception crosses this boundary.  This
+ *     replaces the reference's CUDA_CHECK throw + g_system_error flag
+ *     (src/goldbach.cu:105-114, 496-499).
+ *   - Buffers are caller-owned.  Output pointers are HOST memory unless the
+ *     call's options say `on_device`, in which case they are device
+ *     pointers on the context's GPU.  The library owns all other device
+ *     memory (resident prime tables and work buffers).
+ *   - A context serves one thread at a time, except gb_submit / gb_poll /
+ *     gb_serve_stats, which are thread-safe.
+ *   - "minimal p" of an even n is the smallest prime p <= n/2 with n-p
+ *     prime: the first hit of the ascending scan in
+ *     src/cpu_goldbach.cpp:14-24.  0 means no such p within the bound.
+ */
+#ifndef GB_GB_H
+#define GB_GB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int gb_status;
+#define GB_OK 0
+#define GB_EINVAL (-1)    /* bad argument */
+#define GB_ENOMEM (-2)    /* device memory budget exceeded / allocation failed */
+#define GB_ECUDA (-3)     /* CUDA runtime error */
+#define GB_ETIMEOUT (-4)  /* a bounded device or host wait gave up */
+#define GB_ECANCELED (-5) /* request cancelled / server stopped */
+#define GB_ENODEV (-6)    /* no CUDA device */
+#define GB_EOVERFLOW (-7) /* an internal queue would overflow */
+#define GB_EAGAIN (-8)    /* serving: result not ready yet */
+
+/* Minimal-p histogram: bin k counts n whose minimal p is the k-th prime
+ * (2 -> bin 0, 3 -> 1, 5 -> 2, ...); minimal p of index >= GB_HIST_BINS-1
+ * lands in the last bin.  Failures are counted separately. */
+#define GB_HIST_BINS 4096
+
+/* Phase-2 bound of the reference (PHASE2_SIEVE_LIMIT, src/goldbach.cu:316). */
+#define GB_PHASE2_LIMIT_DEFAULT 100000000ULL
+/* P_SMALL cap of the reference (MAX_P_SMALL, src/goldbach.cu:597). */
+#define GB_P_SMALL_MAX 4000000000ULL
+
+typedef struct gb_ctx gb_ctx;
+
+typedef struct gb_config {
+  /* Device memory the context may hold, in bytes (0 = what the device
+   * reports free at creation).  Allocations beyond it fail with GB_ENOMEM,
+   * like the VRAM guard of src/goldbach.cu:505-541. */
+  uint64_t device_mem_budget;
+  /* Prime tables are built lazily and grow on demand; these pre-size them. */
+  uint64_t max_n;        /* sieving primes up to isqrt(max_n)+1 (0: grow) */
+  uint64_t cand_limit;   /* candidate primes up to this bound (0: 1e8)    */
+} gb_config;
+
+/* Number of visible CUDA devices (0 if none or no driver). */
+int gb_device_count(void);
+/* Name and total memory of a device, as reported by
+ * validate_hardware_and_limits (src/goldbach.cu:527-540). */
+gb_status gb_device_info(int device, char* name, size_t name_len, uint64_t* total_mem);
+/* Device bytes a context with this configuration holds once its tables are
+ * built (the requirement the VRAM guard of src/goldbach.cu:505-541 checks). */
+uint64_t gb_estimate_device_bytes(const gb_config* cfg);
+
+/* Creates a context on `device` (src/goldbach.cu:388-417: stream, resident
+ * tables).  cfg may be NULL. */
+gb_status gb_create(int device, const gb_config* cfg, gb_ctx** out);
+void gb_destroy(gb_ctx* ctx);
+const char* gb_strerror(gb_status st);
+/* Human-readable detail of the last error on this context ("" if none). */
+const char* gb_last_error(const gb_ctx* ctx);
+/* Device bytes the context holds now, and its budget. */
+gb_status gb_mem_info(const gb_ctx* ctx, uint64_t* held, uint64_t* budget);
+
+/* -------------------------------------------------------------------------
+ * Range verification: every even n in [start, limit].
+ * Replaces run_gpu_worker's segment loop (src/goldbach.cu:420-485): the
+ * tiled sieve (:198-259), Phase 1 (:288-311), the unverified count
+ * (:184-195) and the host Phase 2 (:362-373), all on the device.
+ * ---------------------------------------------------------------------- */
+typedef struct gb_range_opts {
+  uint64_t seg_size;      /* even n per reported segment (SEG_SIZE; 0: 1e7) */
+  uint64_t p_small;       /* Phase-1 bound P_SMALL (0: 1e6); the fallback
+                             count is #{n : minimal p > p_small}           */
+  uint64_t phase2_limit;  /* Phase-2 bound (0: 1e8); n with no p <=
+                             max(p_small, phase2_limit) is a failure       */
+  uint32_t chunk_evens;   /* even n per CTA window (0: auto; power of 2,
+                             2^12..2^20)                                   */
+  uint32_t halo;          /* q-window halo in numbers (0: auto; multiple of
+                             64, 128..2^17); primes p < halo are searched
+                             in shared memory, larger ones on the Phase-2
+                             path                                          */
+  uint32_t shard_index;   /* process only segments s with                   */
+  uint32_t shard_count;   /*   s % shard_count == shard_index (0/1: all)    */
+  int on_device;          /* outputs below are device pointers              */
+  void* stream;           /* cudaStream_t to launch on (NULL: ctx stream)   */
+} gb_range_opts;
+
+typedef struct gb_range_result {
+  uint64_t checked;          /* even n examined                            */
+  uint64_t verified;         /* n with a minimal p within the bound        */
+  uint64_t phase2_fallbacks; /* "Phase 2 fallbacks" of src/goldbach.cu:799 */
+  uint64_t failures;         /* n with no partition within the bound       */
+  uint64_t first_failure_n;  /* smallest failing n (0: none)               */
+  uint64_t max_minp;         /* largest minimal p seen                     */
+  uint64_t num_segments;     /* segments of seg_size even n in the range   */
+  uint64_t queued;           /* n resolved on the Phase-2 device path      */
+  uint64_t kernel_launches;  /* device kernels this call launched          */
+  double device_ms;          /* device time of the call (CUDA events)      */
+  double kernel_ms;          /* device time of the sieve+search kernel     */
+} gb_range_result;
+
+typedef struct gb_range_out {
+  uint32_t* verified_bits;  /* ceil(count/32) words, bit j <-> start+2j      */
+  uint32_t* min_p;          /* count entries: minimal p per n               */
+  uint64_t* minp_hist;      /* GB_HIST_BINS                                 */
+  uint32_t* seg_fallbacks;  /* num_segments: fallbacks per segment          */
+  uint32_t* seg_failures;   /* num_segments: failures per segment           */
+  uint64_t* seg_hist;       /* num_segments x GB_HIST_BINS                  */
+} gb_range_out;
+
+/* Number of segments [start, limit] splits into for a seg_size. */
+uint64_t gb_num_segments(uint64_t start, uint64_t limit, uint64_t seg_size);
+
+/* out may be NULL (summary only).  start/limit follow the reference's
+ * normalisation (src/goldbach.cu:593-609): limit odd -> limit-1, start < 4
+ * -> 4, start odd -> start+1; start must then be <= limit. */
+gb_status gb_verify_range(gb_ctx* ctx, uint64_t start, uint64_t limit,
+                          const gb_range_opts* opts, gb_range_result* res,
+                          const gb_range_out* out);
+
+/* -------------------------------------------------------------------------
+ * Odd-only prime bitset of a window (the GPU sieve on its own): bit i of
+ * `words` <-> odd q_lo + 2*i is prime.  Replaces build_prime_bitset
+ * (src/prime_bitset.cpp:21-97) and the tiled sieve's output layout
+ * (src/goldbach.cu:198-259) with a race-free sm_100a sieve.  q_lo odd.
+ * ---------------------------------------------------------------------- */
+gb_status gb_sieve_bitset(gb_ctx* ctx, uint64_t q_lo, uint64_t nbits,
+                          uint32_t* words, int on_device, void* stream);
+
+/* Primes <= limit in ascending order (2 first), from the device prime
+ * table.  *count receives the number of primes; `primes` (cap entries,
+ * nullable) receives them.  Replaces generate_cpu_primes
+ * (src/goldbach.cu:318-331). */
+gb_status gb_primes_upto(gb_ctx* ctx, uint64_t limit, uint32_t* primes,
+                         uint64_t cap, uint64_t* count);
+
+/* Deterministic 64-bit primality (Montgomery Miller-Rabin, bases 2, 325,
+ * 9375, 28178, 450775, 9780504, 1795265022) for a batch.  Replaces
+ * gpu_is_prime_miller_rabin (src/goldbach.cu:144-158) and
+ * is_prime_miller_rabin (src/single_check.cu:67-88). */
+gb_status gb_is_prime_batch(gb_ctx* ctx, const uint64_t* n, size_t count,
+                            uint8_t* out, int on_device, void* stream);
+
+/* -------------------------------------------------------------------------
+ * Batched single-n checks: for each even n >= 4 the minimal p and q = n-p.
+ * Replaces check_single / goldbach_single_kernel (src/single_check.cu:
+ * 95-282), which returns the first-finishing partition, with the minimal
+ * one.  p = q = 0 for an n without a partition with p <= p_limit.
+ * ---------------------------------------------------------------------- */
+typedef struct gb_single_opts {
+  uint64_t p_limit;  /* candidate bound (0: 1e8)                          */
+  int on_device;     /* n / p_out / q_out are device pointers             */
+  void* stream;
+} gb_single_opts;
+
+typedef struct gb_single_result {
+  uint64_t found;           /* queries with a partition                   */
+  uint64_t max_p;           /* largest minimal p                          */
+  uint64_t kernel_launches;
+  double device_ms;
+} gb_single_result;
+
+gb_status gb_check_single_batch(gb_ctx* ctx, const uint64_t* n, size_t count,
+                                uint64_t* p_out, uint64_t* q_out,
+                                const gb_single_opts* opts,
+                                gb_single_result* res);
+
+/* -------------------------------------------------------------------------
+ * Batched windows: many independent ranges of consecutive even n.
+ * ---------------------------------------------------------------------- */
+typedef struct gb_window {
+  uint64_t start; /* first even n (>= 4)      */
+  uint64_t count; /* number of even n (>= 1)  */
+} gb_window;
+
+#define GB_WINDOWS_PERSISTENT 0 /* one persistent launch, device work queue */
+#define GB_WINDOWS_PLAIN 1      /* one pipeline of launches per window      */
+
+typedef struct gb_windows_opts {
+  int mode;               /* GB_WINDOWS_PERSISTENT or GB_WINDOWS_PLAIN      */
+  uint32_t chunk_evens;   /* 0: autotuned                                   */
+  uint32_t halo;          /* 0: auto                                        */
+  uint64_t phase2_limit;  /* 0: 1e8                                         */
+  int on_device;          /* windows / min_p / res are device pointers      */
+  void* stream;
+} gb_windows_opts;
+
+typedef struct gb_window_result {
+  uint64_t verified;
+  uint64_t failures;
+  uint64_t max_minp;
+  uint64_t minp_sum; /* sum of minimal p over the window (checksum)        */
+} gb_window_result;
+
+typedef struct gb_windows_summary {
+  uint64_t total_n;
+  uint64_t failures;
+  uint64_t kernel_launches;
+  double device_ms;
+} gb_windows_summary;
+
+/* min_p_concat (nullable) receives the minimal p of every n, window after
+ * window (sum of counts entries). */
+gb_status gb_verify_windows(gb_ctx* ctx, const gb_window* w, size_t count,
+                            const gb_windows_opts* opts, gb_window_result* res,
+                            uint32_t* min_p_concat, gb_windows_summary* sum);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GB_GB_H */

@@ -1,0 +1,67 @@
+"""The CLIs on a GPU: the reference's tests/validation_gpu.sh and
+tests/validation.sh cases that need a device, plus the failure path."""
+import os
+import re
+import subprocess
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+BIN = os.path.join(os.path.dirname(__file__), "..", "goldbach-gpu_b200", "bin")
+
+
+def run(prog, *args, timeout=300):
+    p = subprocess.run([os.path.join(BIN, prog), *map(str, args)], capture_output=True,
+                       text=True, timeout=timeout)
+    return p.returncode, p.stdout + p.stderr
+
+
+def test_basic_run_1e9():  # validation_gpu.sh Test 1.1
+    rc, out = run("goldbach", 1000000000, "--seg-size=1000000", "--p-small=100000",
+                  "--batch-size=100000")
+    assert rc == 0, out
+    assert "satisfy Goldbach. ✓" in out and "Phase 2 fallbacks      : 0" in out
+    assert re.search(r"Total computation time : [0-9.e+-]+ seconds", out)
+
+
+def test_progress_flag():  # Test 1.2
+    rc, out = run("goldbach", 20000000000, "--seg-size=10000000", "--p-small=1000000",
+                  "--batch-size=1000000", "--progress")
+    assert rc == 0 and "[Progress]" in out and "satisfy Goldbach. ✓" in out, out
+
+
+def test_custom_start():  # Test 1.3
+    rc, out = run("goldbach", 1000000000, "--seg-size=1000000", "--p-small=100000",
+                  "--batch-size=100000", "--start=1000000")
+    assert rc == 0 and "Checking range : [1000000" in out and "satisfy Goldbach. ✓" in out
+
+
+def test_more_gpus_than_available():  # Test 3.6
+    rc, out = run("goldbach", 100000000, "--gpus=64")
+    assert "Requested" in out and "available" in out and "Using" in out
+    assert rc == 0
+
+
+def test_vram_guard():  # Test 3.5 (memory budget forced small)
+    rc, out = run("goldbach", 100000000000, "--seg-size=100000000000", "--device-mem-mb=16")
+    assert rc == 1 and "insufficient VRAM" in out
+
+
+def test_failure_is_reported():
+    rc, out = run("goldbach", 1000, "--seg-size=100", "--p-small=3", "--phase2-limit=3")
+    assert rc == 1 and "[!] Goldbach FAILED at n = 12" in out, out
+
+
+def test_json_summary():
+    rc, out = run("goldbach", 10000000, "--json")
+    assert rc == 0
+    m = re.search(r'\{"start": 4, "limit": 10000000, "checked": (\d+)', out)
+    assert m and int(m.group(1)) == 4999999
+
+
+def test_single_check_1e12():  # validation.sh Test 1.2
+    rc, out = run("single_check", 1000000000000)
+    assert rc == 0 and "Goldbach holds. ✓" in out
+    m = re.search(r"1000000000000 = (\d+) \+ (\d+)", out)
+    assert m and int(m.group(1)) + int(m.group(2)) == 10**12
+    assert int(m.group(1)) <= 194267
