@@ -282,7 +282,7 @@ def main():
     # every chunk window incl. its halo), written once and read once if it
     # were staged through HBM; the fused kernel keeps it in shared memory.
     halo = args.halo or 32768
-    chunk = args.chunk or (1 << 18)
+    chunk = args.chunk or (1 << 19)
     n_mine = sum(min(args.seg_size, total - s * args.seg_size) for s in range(rank, nseg, world))
     chunks = sum(math.ceil(min(args.seg_size, total - s * args.seg_size) / chunk)
                  for s in range(rank, nseg, world))

@@ -365,7 +365,7 @@ gb_status gb_verify_range(gb_ctx* c, uint64_t start, uint64_t limit, const gb_ra
   if (H < 128 || H > (1u << 17) || (H & 63)) return fail(c, GB_EINVAL, "halo must be a multiple of 64 in [128, 2^17]");
   uint32_t NE = o.chunk_evens;
   if (!NE) {
-    NE = 1u << 18;
+    NE = 1u << 19;
     while (NE > 8192 && NE / 2 >= count) NE >>= 1;
   }
   if (NE < 8192 || NE > (1u << 20) || (NE & (NE - 1)))

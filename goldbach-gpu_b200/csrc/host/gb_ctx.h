@@ -49,7 +49,7 @@ namespace gb {
 
 constexpr uint64_t kHostPrimeLimit = 1ull << 22;
 // primes searched word-parallel (lockstep) before the per-n tail
-constexpr uint64_t kLockPrimes = 64;
+constexpr uint64_t kLockPrimes = 128;
 
 gb_status fail(gb_ctx* c, gb_status st, const std::string& msg);
 gb_status cuda_fail(gb_ctx* c, cudaError_t e, const char* what);

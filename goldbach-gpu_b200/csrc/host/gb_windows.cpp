@@ -38,7 +38,7 @@ extern "C" gb_status gb_verify_windows(gb_ctx* c, const gb_window* w, size_t cou
   if (count > 0xffffffffull) return fail(c, GB_EINVAL, "too many windows");
   const uint32_t H = o.halo ? o.halo : 32768u;
   if (H < 128 || H > (1u << 17) || (H & 63)) return fail(c, GB_EINVAL, "halo must be a multiple of 64 in [128, 2^17]");
-  const uint32_t NE = o.chunk_evens ? o.chunk_evens : (1u << 18);
+  const uint32_t NE = o.chunk_evens ? o.chunk_evens : (1u << 19);
   if (NE < 8192 || NE > (1u << 20) || (NE & (NE - 1)))
     return fail(c, GB_EINVAL, "chunk_evens must be a power of two in [2^13, 2^20]");
   const uint64_t p_lim = o.phase2_limit ? o.phase2_limit : GB_PHASE2_LIMIT_DEFAULT;

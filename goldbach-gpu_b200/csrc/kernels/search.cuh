@@ -36,15 +36,6 @@ struct LaneAcc {
   uint64_t psum;  // sum of minimal p
 };
 
-__device__ __forceinline__ void record_failure(const SearchParams& s, const Chunk& c,
-                                               uint64_t idx, uint64_t n, LaneAcc& acc) {
-  acc.fb++;
-  atomicAdd(&s.ctr[kCtrFailures], 1ull);
-  atomicMin(&s.ctr[kCtrFirstFail], (unsigned long long)n);
-  if (s.unit_failures) atomicAdd(&s.unit_failures[c.unit], 1u);
-  if (s.vbits) atomicAnd(&s.vbits[idx >> 5], ~(1u << (idx & 31)));
-}
-
 __device__ __forceinline__ void record_found_k(const SearchParams& s, uint32_t* HIST, uint32_t k,
                                                uint32_t p, uint64_t unit, LaneAcc& acc) {
   if (k < kSmemHistBins) {
@@ -61,14 +52,18 @@ __device__ __forceinline__ void record_found_k(const SearchParams& s, uint32_t* 
 
 // Finishes one n = A + 2j already tested against the primes of index < k:
 // scalar scan over the remaining window primes, then the Phase-2 queue
-// (minimal p >= H) or a failure (no p <= min(n/2, p_lim)).
+// (minimal p >= H) or a failure (no p <= min(n/2, p_lim)).  Returns the
+// minimal p found here (0 if none) in the low 32 bits and 1 in bit 32 when
+// the n counts as a Phase-2 fallback.  Arguments are passed by value so
+// that the caller's accumulators stay in registers.
 template <bool MINP>
-__device__ __noinline__ void tail_one(const SearchParams& s, const uint32_t* __restrict__ Q,
-                                      const uint16_t* __restrict__ SOFF, uint32_t* HIST,
-                                      uint32_t k, uint32_t j, const Chunk& c, LaneAcc& acc) {
-  const uint64_t n = c.A + 2ull * j;
+__device__ __noinline__ uint64_t tail_one(const SearchParams& s, const uint32_t* __restrict__ Q,
+                                          const uint16_t* __restrict__ SOFF, uint32_t* HIST,
+                                          uint32_t k, uint32_t j, uint64_t A, uint64_t base_idx,
+                                          uint64_t unit) {
+  const uint64_t n = A + 2ull * j;
   const uint64_t half = n >> 1;
-  const uint64_t idx = c.base_idx + j;
+  const uint64_t idx = base_idx + j;
   const uint32_t H1 = s.halo - 1;
   uint32_t kk = k;
   for (; kk < s.nsearch; ++kk) {
@@ -77,24 +72,34 @@ __device__ __noinline__ void tail_one(const SearchParams& s, const uint32_t* __r
     if (p > half) break;
     const uint32_t bit = off + j;
     if ((Q[bit >> 5] >> (bit & 31)) & 1u) {
-      record_found_k(s, HIST, kk, p, c.unit, acc);
+      if (kk < kSmemHistBins) {
+        atomicAdd(&HIST[kk], 1u);
+      } else {
+        const uint32_t bin = kk < GB_HIST_BINS - 1 ? kk : GB_HIST_BINS - 1;
+        if (s.hist) atomicAdd(&s.hist[bin], 1ull);
+        if (s.unit_hist) atomicAdd(&s.unit_hist[unit * GB_HIST_BINS + bin], 1ull);
+      }
       if (MINP) s.minp[idx] = p;
-      return;
+      return (uint64_t)p | ((uint64_t)(kk >= s.kfb) << 32);
     }
   }
   const uint64_t lim = half < s.p_lim ? half : s.p_lim;
   if (kk < s.nsearch || kk >= s.nprimes || s.primes[kk] > lim) {
-    record_failure(s, c, idx, n, acc);
-    return;
+    atomicAdd(&s.ctr[kCtrFailures], 1ull);
+    atomicMin(&s.ctr[kCtrFirstFail], (unsigned long long)n);
+    if (s.unit_failures) atomicAdd(&s.unit_failures[unit], 1u);
+    if (s.vbits) atomicAnd(&s.vbits[idx >> 5], ~(1u << (idx & 31)));
+    return 1ull << 32;
   }
   const unsigned long long slot = atomicAdd(&s.ctr[kCtrQueue], 1ull);
   if (slot < s.queue_cap) {
     s.queue[slot].n = n;
     s.queue[slot].idx = idx;
-    s.queue[slot].unit = c.unit;
+    s.queue[slot].unit = unit;
   } else {
     s.ctr[kCtrQueueOvf] = 1ull;
   }
+  return 0;  // the Phase-2 kernel accounts for it
 }
 
 // One warp task: words [task*256, task*256+256) of the chunk; lane l owns
@@ -194,14 +199,20 @@ __device__ __forceinline__ void search_task(const SearchParams& s, const uint32_
       acc.psum += (uint64_t)cnt * p;
     }
   }
-  // Tail: the n left after the lockstep primes, one at a time.
-#pragma unroll 1
+  // Tail: the n left after the lockstep primes, one at a time.  (Unrolled:
+  // a runtime index into U would move the whole array to local memory.)
+#pragma unroll
   for (int i = 0; i < kWT; ++i) {
     uint32_t u = U[i];
     while (u) {
       const int b = __ffs(u) - 1;
       u &= u - 1;
-      tail_one<MINP>(s, Q, SOFF, HIST, k, 32 * (wbase + 32 * i) + b, c, acc);
+      const uint64_t r =
+          tail_one<MINP>(s, Q, SOFF, HIST, k, 32 * (wbase + 32 * i) + b, c.A, c.base_idx, c.unit);
+      const uint32_t p = (uint32_t)r;
+      acc.fb += (uint32_t)(r >> 32);
+      if (p > acc.maxp) acc.maxp = p;
+      acc.psum += p;
     }
   }
 }

@@ -341,6 +341,39 @@ int gbo_minp_range(uint64_t start, uint64_t count, uint64_t p_limit,
   return err ? -1 : 0;
 }
 
+int gbo_minp_windows(const uint64_t* start, const uint64_t* count, size_t nwin,
+                     uint64_t p_limit, uint32_t* minp_out, int nthreads) {
+  uint64_t qmax = 0, nblk = 0;
+  for (size_t i = 0; i < nwin; i++) {
+    if (start[i] < 4 || (start[i] & 1) || !count[i]) return -1;
+    uint64_t last = start[i] + 2 * (count[i] - 1);
+    if (last > qmax) qmax = last;
+    nblk += (count[i] + ORACLE_BLOCK - 1) / ORACLE_BLOCK;
+  }
+  uint64_t need = p_limit > ORACLE_HALO ? p_limit : ORACLE_HALO;
+  if (gbo_isqrt(qmax) > need) need = gbo_isqrt(qmax);
+  size_t tmp = 0;
+  prime_cache(need, &tmp); /* build the shared tables once, before the threads */
+  uint64_t* bw = (uint64_t*)malloc(nblk * sizeof(uint64_t) * 3);
+  if (!bw) return -1;
+  uint64_t b = 0, off = 0;
+  for (size_t i = 0; i < nwin; i++) {
+    for (uint64_t j0 = 0; j0 < count[i]; j0 += ORACLE_BLOCK, b++) {
+      bw[3 * b] = start[i] + 2 * j0;
+      bw[3 * b + 1] = count[i] - j0 < ORACLE_BLOCK ? count[i] - j0 : ORACLE_BLOCK;
+      bw[3 * b + 2] = off + j0;
+    }
+    off += count[i];
+  }
+  int err = 0;
+  int nt = pick_threads(nthreads);
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 1) reduction(| : err)
+  for (long long k = 0; k < (long long)nblk; k++)
+    err |= gbo_minp_range(bw[3 * k], bw[3 * k + 1], p_limit, minp_out + bw[3 * k + 2], 1) != 0;
+  free(bw);
+  return err ? -1 : 0;
+}
+
 /* ---------------------------------------------------------------------- */
 uint64_t gbo_single_minp(uint64_t n, uint64_t p_limit) {
   if (n < 4 || (n & 1)) return 0;

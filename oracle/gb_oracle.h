@@ -72,6 +72,12 @@ uint64_t gbo_phase2_minp(uint64_t n, uint64_t limit);
 int gbo_minp_range(uint64_t start, uint64_t count, uint64_t p_limit,
                    uint32_t* minp_out, int nthreads);
 
+/* gbo_minp_range over many windows at once: window i covers start[i] +
+ * 2j, j < count[i]; results are concatenated in window order.  Windows are
+ * split into blocks and all blocks run in parallel (nthreads). */
+int gbo_minp_windows(const uint64_t* start, const uint64_t* count, size_t nwin,
+                     uint64_t p_limit, uint32_t* minp_out, int nthreads);
+
 /* Minimal prime p with n-p prime for one even n >= 4 (n = 4 -> 2), primes
  * ascending from 2 up to min(p_limit, n/2), q tested by gbo_mr7; 0 if none.
  * This is the answer single-n queries must return (a minimal refinement of

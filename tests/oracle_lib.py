@@ -38,6 +38,7 @@ class Oracle:
         L.gbo_phase2_minp.restype = u64
         L.gbo_phase2_minp.argtypes = [u64, u64]
         L.gbo_minp_range.argtypes = [u64, u64, u64, C.c_void_p, C.c_int]
+        L.gbo_minp_windows.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, u64, C.c_void_p, C.c_int]
         L.gbo_single_minp.restype = u64
         L.gbo_single_minp.argtypes = [u64, u64]
         L.gbo_single_minp_batch.argtypes = [C.c_void_p, C.c_size_t, u64, C.c_void_p, C.c_int]
@@ -76,6 +77,14 @@ class Oracle:
         a = np.zeros(count, np.uint32)
         assert self.L.gbo_minp_range(start, count, p_limit, a.ctypes.data, threads) == 0
         return a
+
+    def minp_windows(self, starts, counts, p_limit=10**8, threads=0):
+        starts = np.ascontiguousarray(starts, dtype=np.uint64)
+        counts = np.ascontiguousarray(counts, dtype=np.uint64)
+        out = np.zeros(int(counts.sum()), np.uint32)
+        assert self.L.gbo_minp_windows(starts.ctypes.data, counts.ctypes.data, len(starts), p_limit,
+                                       out.ctypes.data, threads) == 0
+        return out
 
     def single_minp(self, ns, p_limit=10**8, threads=0):
         ns = np.ascontiguousarray(ns, dtype=np.uint64)
