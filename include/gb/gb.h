@@ -189,6 +189,32 @@ gb_status gb_check_single_batch(gb_ctx* ctx, const uint64_t* n, size_t count,
                                 gb_single_result* res);
 
 /* -------------------------------------------------------------------------
+ * Batched single-n checks that allocate no device memory.
+ *
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * code running while a stream is captured into a CUDA graph, code living in
+ * another framework's memory pool, or a real-time loop that must not touch
+ * the allocator.  No context is needed and nothing is allocated: n, p_out
+ * and q_out are device buffers on the current device (count entries each);
+ * the kernel's counters and candidate primes live in a fixed file-scope
+ * device array of about 26 KB that every GPU which loads this library holds
+ * until the process exits.
+ *   - p_limit bounds the candidate p (0: GB_NOALLOC_P_LIMIT, the largest
+ *     prime below 2^16, which is the reach of the fixed table); a larger
+ *     p_limit returns GB_EINVAL.  Results equal gb_check_single_batch with
+ *     the same p_limit.
+ *   - The first call on each device builds the table and synchronises
+ *     `stream`; make that first call before any stream capture.
+ *   - Later calls are asynchronous on `stream` (cudaStream_t, NULL: legacy
+ *     default stream); the counters are cleared on every call.
+ *   - All calls share the one array: calls that overlap on the GPU (two
+ *     streams, two threads) race.  Serialise them.
+ * ---------------------------------------------------------------------- */
+#define GB_NOALLOC_P_LIMIT 65521ULL
+gb_status gb_check_single_batch_noalloc(const uint64_t* n, size_t count, uint64_t* p_out,
+                                        uint64_t* q_out, uint64_t p_limit, void* stream);
+
+/* -------------------------------------------------------------------------
  * Batched windows: many independent ranges of consecutive even n.
  * ---------------------------------------------------------------------- */
 typedef struct gb_window {
