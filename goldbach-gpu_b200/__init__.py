@@ -88,6 +88,36 @@ class WindowsSummary(C.Structure):
                 ("device_ms", C.c_double)]
 
 
+class Request(C.Structure):
+    _fields_ = [("kind", i32), ("a", u64), ("count", u64), ("arrival_ns", u64)]
+
+
+class Response(C.Structure):
+    _fields_ = [("status", i32), ("kind", i32), ("p", u64), ("q", u64), ("verified", u64),
+                ("failures", u64), ("max_minp", u64), ("minp_sum", u64), ("latency_us", C.c_double),
+                ("lane", u32), ("batch", u32)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class ServeOpts(C.Structure):
+    _fields_ = [("max_n", u64), ("max_single_batch", u32), ("max_range_batch", u32),
+                ("range_arena_bytes", u64), ("small_range", u64)]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [("submitted", u64), ("completed", u64), ("pending", u64), ("rejected", u64),
+                ("batches_single", u64), ("batches_range", u64), ("p50_us", C.c_double),
+                ("p99_us", C.c_double), ("max_us", C.c_double), ("mean_us", C.c_double),
+                ("elapsed_s", C.c_double), ("completed_per_s", C.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+GB_REQ_SINGLE, GB_REQ_RANGE = 0, 1
+
 _lib = None
 
 
@@ -117,6 +147,14 @@ def load(path: str = LIB_PATH):
         "gb_check_single_batch": (i32, [vp, vp, C.c_size_t, vp, vp, P(SingleOpts), P(SingleResult)]),
         "gb_verify_windows": (i32, [vp, P(Window), C.c_size_t, P(WindowsOpts), P(WindowResult),
                                     vp, P(WindowsSummary)]),
+        "gb_now_ns": (u64, []),
+        "gb_probe_peaks": (i32, [vp, P(C.c_double), P(C.c_double)]),
+        "gb_serve_start": (i32, [vp, P(ServeOpts)]),
+        "gb_submit": (i32, [vp, P(Request), C.c_size_t, P(u64)]),
+        "gb_poll": (i32, [vp, u64, P(Response)]),
+        "gb_wait": (i32, [vp, u64, P(Response), u64]),
+        "gb_serve_stats_get": (i32, [vp, P(ServeStats), i32]),
+        "gb_serve_stop": (i32, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name, None)
@@ -290,3 +328,54 @@ class Context:
                                              _ptr(minp), C.byref(s)))
         per = [{f: getattr(res[i], f) for f, _ in WindowResult._fields_} for i in range(nw)]
         return per, minp, {f: getattr(s, f) for f, _ in WindowsSummary._fields_}
+
+    # -- serving ---------------------------------------------------------------
+    def serve_start(self, max_n: int = 0, max_single_batch: int = 0, max_range_batch: int = 0,
+                    range_arena_bytes: int = 0, small_range: int = 0):
+        o = ServeOpts(max_n, max_single_batch, max_range_batch, range_arena_bytes, small_range)
+        self._check(self.L.gb_serve_start(self._h, C.byref(o)))
+
+    def submit(self, kinds, a, counts=None, arrival_ns=None) -> np.ndarray:
+        """Queues requests (kind GB_REQ_SINGLE / GB_REQ_RANGE); returns tickets."""
+        kinds = np.asarray(kinds, dtype=np.int32)
+        a = np.asarray(a, dtype=np.uint64)
+        m = len(kinds)
+        counts = np.ones(m, np.uint64) if counts is None else np.asarray(counts, dtype=np.uint64)
+        arr = np.zeros(m, np.uint64) if arrival_ns is None else np.asarray(arrival_ns, dtype=np.uint64)
+        reqs = np.zeros(m, dtype=[("kind", "<i4"), ("pad", "<i4"), ("a", "<u8"), ("count", "<u8"),
+                                  ("arrival_ns", "<u8")])
+        reqs["kind"], reqs["a"], reqs["count"], reqs["arrival_ns"] = kinds, a, counts, arr
+        t = np.zeros(m, np.uint64)
+        self._check(self.L.gb_submit(self._h, reqs.ctypes.data_as(C.POINTER(Request)), m,
+                                     t.ctypes.data_as(C.POINTER(u64))))
+        return t
+
+    def poll(self, ticket: int):
+        r = Response()
+        st = self.L.gb_poll(self._h, int(ticket), C.byref(r))
+        if st == GB_EAGAIN:
+            return None
+        self._check(st)
+        return r.as_dict()
+
+    def wait(self, ticket: int, timeout_ms: int = 60000):
+        r = Response()
+        self._check(self.L.gb_wait(self._h, int(ticket), C.byref(r), timeout_ms))
+        return r.as_dict()
+
+    def serve_stats(self, reset: bool = False) -> dict:
+        s = ServeStats()
+        self._check(self.L.gb_serve_stats_get(self._h, C.byref(s), int(reset)))
+        return s.as_dict()
+
+    def serve_stop(self):
+        self._check(self.L.gb_serve_stop(self._h))
+
+    def probe_peaks(self) -> tuple[float, float]:
+        """(32-bit ALU ops/s, shared-memory atomicAnd/s) measured on this GPU."""
+        a, m = C.c_double(), C.c_double()
+        self._check(self.L.gb_probe_peaks(self._h, C.byref(a), C.byref(m)))
+        return a.value, m.value
+
+    def now_ns(self) -> int:
+        return self.L.gb_now_ns()

@@ -129,8 +129,13 @@ cudaError_t launch_fallback(const SearchParams& s, int grid, cudaStream_t st);
 
 // kernels/windows.cu: the three stages for all windows (w_only = ~0u) or for
 // one window; grids are chosen by the caller.
+cudaError_t launch_win_nsieve(WinDesc* win, uint32_t nwin, const uint32_t* primes, uint64_t nprimes,
+                              cudaStream_t s);
 cudaError_t launch_window_stages(const WindowsArgs& a, uint32_t w_only, int grid_tile,
                                  int grid_large, int grid_search, cudaStream_t s, int* launches);
+
+// kernels/probe.cu: kind 0 = 32-bit ALU ops/s, 1 = shared-memory atomicAnd/s
+cudaError_t run_probe(int kind, int sm_count, double* ops_per_s, cudaStream_t st);
 
 // kernels/single.cu
 struct SingleArgs {
@@ -145,5 +150,7 @@ struct SingleArgs {
 };
 cudaError_t launch_single(const SingleArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_is_prime(const uint64_t* n, uint64_t count, uint8_t* out, cudaStream_t s);
+cudaError_t launch_segment_reduce(const uint64_t* p, const uint64_t* off, uint32_t nreq,
+                                  unsigned long long* agg, cudaStream_t s);
 
 }  // namespace gb

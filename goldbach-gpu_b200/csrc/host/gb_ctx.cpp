@@ -15,38 +15,43 @@
 
 namespace gb {
 
-gb_status fail(gb_ctx* c, gb_status st, const std::string& msg) {
-  if (c) c->err = msg;
+gb_status fail(Workspace& w, gb_status st, const std::string& msg) {
+  w.err = msg;
   return st;
 }
 
-gb_status cuda_fail(gb_ctx* c, cudaError_t e, const char* what) {
-  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
-  return fail(c, e == cudaErrorMemoryAllocation ? GB_ENOMEM : GB_ECUDA, m);
+gb_status cuda_fail(Workspace& w, cudaError_t e, const char* what) {
+  return fail(w, e == cudaErrorMemoryAllocation ? GB_ENOMEM : GB_ECUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-#define GB_CU(call, what)                              \
-  do {                                                 \
-    cudaError_t e_ = (call);                           \
-    if (e_ != cudaSuccess) return cuda_fail(c, e_, what); \
+#define GB_CU(call, what)                                 \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return cuda_fail(w, e_, what); \
   } while (0)
 
-gb_status dev_alloc(gb_ctx* c, void** p, size_t bytes) {
+gb_status dev_alloc(gb_ctx* c, void** p, size_t bytes, std::string* err) {
   *p = nullptr;
   if (bytes == 0) bytes = 16;
+  std::lock_guard<std::mutex> lk(c->alloc_mu);
   if (c->held + bytes > c->budget) {
-    char buf[256];
-    snprintf(buf, sizeof buf,
-             "insufficient VRAM: required %llu MB more, budget %llu MB, held %llu MB",
-             (unsigned long long)(bytes >> 20), (unsigned long long)(c->budget >> 20),
-             (unsigned long long)(c->held >> 20));
-    return fail(c, GB_ENOMEM, buf);
+    if (err) {
+      char buf[256];
+      snprintf(buf, sizeof buf,
+               "insufficient VRAM: required %llu MB more, budget %llu MB, held %llu MB",
+               (unsigned long long)(bytes >> 20), (unsigned long long)(c->budget >> 20),
+               (unsigned long long)(c->held >> 20));
+      *err = buf;
+    }
+    return GB_ENOMEM;
   }
   cudaError_t e = cudaMalloc(p, bytes);
   if (e != cudaSuccess) {
     cudaGetLastError();
     *p = nullptr;
-    return cuda_fail(c, e, "cudaMalloc");
+    if (err) *err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+    return GB_ENOMEM;
   }
   c->held += bytes;
   c->allocs[*p] = bytes;
@@ -55,12 +60,55 @@ gb_status dev_alloc(gb_ctx* c, void** p, size_t bytes) {
 
 void dev_free(gb_ctx* c, void* p) {
   if (!p) return;
+  std::lock_guard<std::mutex> lk(c->alloc_mu);
   auto it = c->allocs.find(p);
   if (it != c->allocs.end()) {
     c->held -= it->second;
     c->allocs.erase(it);
   }
   cudaFree(p);
+}
+
+gb_status Temps::get(size_t bytes, void** p, Workspace& w) {
+  if (arena) {
+    *p = arena->take(bytes);
+    return *p ? GB_OK : fail(w, GB_ENOMEM, "serving arena exhausted");
+  }
+  gb_status st = dev_alloc(c, p, bytes, &w.err);
+  if (st == GB_OK) owned.push_back(*p);
+  return st;
+}
+
+void Temps::release() {
+  for (void* p : owned) dev_free(c, p);
+  owned.clear();
+}
+
+gb_status ws_init(gb_ctx* c, Workspace& w, uint32_t queue_cap) {
+  gb_status st;
+  if ((st = dev_alloc(c, (void**)&w.ctr, kCtrCount * 8, &w.err)) != GB_OK ||
+      (st = dev_alloc(c, (void**)&w.hist, GB_HIST_BINS * 8, &w.err)) != GB_OK ||
+      (st = dev_alloc(c, (void**)&w.queue, (size_t)queue_cap * sizeof(QEntry), &w.err)) != GB_OK)
+    return st;
+  w.queue_cap = queue_cap;
+  if (cudaEventCreate(&w.ev0) != cudaSuccess || cudaEventCreate(&w.ev1) != cudaSuccess ||
+      cudaEventCreate(&w.ek0) != cudaSuccess || cudaEventCreate(&w.ek1) != cudaSuccess)
+    return fail(w, GB_ECUDA, "cudaEventCreate");
+  return GB_OK;
+}
+
+void ws_free(gb_ctx* c, Workspace& w) {
+  dev_free(c, w.ctr);
+  dev_free(c, w.hist);
+  dev_free(c, w.queue);
+  w.ctr = nullptr;
+  w.hist = nullptr;
+  w.queue = nullptr;
+  for (cudaEvent_t* e : {&w.ev0, &w.ev1, &w.ek0, &w.ek1})
+    if (*e) {
+      cudaEventDestroy(*e);
+      *e = nullptr;
+    }
 }
 
 uint64_t isqrt_u64(uint64_t n) {  // exact floor(sqrt(n)), src/goldbach.cu:637-646
@@ -76,70 +124,76 @@ static uint64_t pi_upper(uint64_t x) {
   return (uint64_t)(1.2551 * (double)x / std::log((double)x)) + 64;
 }
 
-gb_status count_le(gb_ctx* c, uint64_t x, uint64_t* out) {
+gb_status count_le(gb_ctx* c, Workspace& w, uint64_t x, uint64_t* out) {
   if (x >= c->primes_limit && c->primes_limit) {
     *out = c->nprimes;
     return GB_OK;
   }
   if (x <= kHostPrimeLimit || c->nprimes == c->h_primes.size()) {
-    *out = std::upper_bound(c->h_primes.begin(), c->h_primes.end(), (uint32_t)std::min<uint64_t>(x, 0xffffffffu)) -
+    *out = std::upper_bound(c->h_primes.begin(), c->h_primes.end(),
+                            (uint32_t)std::min<uint64_t>(x, 0xffffffffu)) -
            c->h_primes.begin();
     return GB_OK;
   }
-  // binary search over the device table
-  uint64_t lo = c->h_primes.size(), hi = c->nprimes;
-  while (lo < hi) {
-    uint64_t mid = lo + (hi - lo) / 2;
-    uint32_t v = 0;
-    GB_CU(cudaMemcpy(&v, c->d_primes + mid, 4, cudaMemcpyDeviceToHost), "count_le");
-    if (v <= x) lo = mid + 1;
-    else hi = mid;
+  // the host sample brackets x within one block of kSampleStride primes;
+  // one copy of that block finishes the count
+  const uint64_t b = std::upper_bound(c->h_sample.begin(), c->h_sample.end(),
+                                      (uint32_t)std::min<uint64_t>(x, 0xffffffffu)) -
+                     c->h_sample.begin();  // samples <= x
+  if (b == 0) {
+    *out = 0;
+    return GB_OK;
   }
-  *out = lo;
+  const uint64_t lo = (b - 1) * kSampleStride;
+  const uint64_t len = std::min<uint64_t>(kSampleStride, c->nprimes - lo);
+  std::vector<uint32_t> blk(len);
+  GB_CU(cudaMemcpy(blk.data(), c->d_primes + lo, len * 4, cudaMemcpyDeviceToHost), "count_le");
+  *out = lo + (std::upper_bound(blk.begin(), blk.end(), (uint32_t)std::min<uint64_t>(x, 0xffffffffu)) -
+               blk.begin());
   return GB_OK;
 }
 
 // Builds (or grows) the resident prime table to cover [2, limit] on the
 // device: the wheel alone is exact below 71^2, and each further stage
 // sieves [3, L^2] with the primes <= L of the previous one.
-gb_status ensure_primes(gb_ctx* c, uint64_t limit) {
+gb_status ensure_primes(gb_ctx* c, Workspace& w, uint64_t limit) {
   if (limit <= c->primes_limit) return GB_OK;
+  if (limit > 0xffffffffull && limit <= 0x100000002ull) limit = 0xffffffffull;  // sqrt of n near 2^64
+  if (limit <= c->primes_limit) return GB_OK;
+  if (c->server)  // the serving lanes read the tables without a lock
+    return fail(w, GB_EINVAL, "prime tables are frozen while serving: size them in gb_serve_start");
   uint64_t target = std::max<uint64_t>(limit, 1ull << 22);
-  if (target > 0xffffffffull) return fail(c, GB_EINVAL, "prime table limit above 2^32");
+  if (target > 0xffffffffull) return fail(w, GB_EINVAL, "prime table limit above 2^32");
   if (!(target & 1)) target++;  // odd top
   if (target > 0xffffffffull) target = 0xfffffffbull;
   const uint64_t cap = pi_upper(target);
-  uint32_t* primes = nullptr;
-  uint64_t* magic = nullptr;
-  uint32_t* bits = nullptr;
-  uint32_t* blocks = nullptr;
-  unsigned long long* total = nullptr;
   const uint64_t nbits_max = (target - 3) / 2 + 1;
   const size_t nblk = compact_scratch_blocks(nbits_max);
+  uint32_t* primes = nullptr;
+  uint64_t* magic = nullptr;
+  Temps t(c, nullptr);
+  uint32_t *bits, *blocks;
+  unsigned long long* total;
   gb_status st;
-  auto cleanup = [&]() {
-    dev_free(c, bits);
-    dev_free(c, blocks);
-    dev_free(c, total);
-  };
-  if ((st = dev_alloc(c, (void**)&primes, cap * 4)) != GB_OK) return st;
-  if ((st = dev_alloc(c, (void**)&magic, cap * 8)) != GB_OK) {
-    dev_free(c, primes);
-    return st;
-  }
-  if ((st = dev_alloc(c, (void**)&bits, ((nbits_max + 31) / 32 + 4) * 4)) != GB_OK ||
-      (st = dev_alloc(c, (void**)&blocks, (nblk + 1) * 4)) != GB_OK ||
-      (st = dev_alloc(c, (void**)&total, 8)) != GB_OK) {
-    cleanup();
+  if ((st = dev_alloc(c, (void**)&primes, cap * 4, &w.err)) != GB_OK) return st;
+  if ((st = dev_alloc(c, (void**)&magic, cap * 8, &w.err)) != GB_OK ||
+      (st = t.get(((nbits_max + 31) / 32 + 4) * 4, (void**)&bits, w)) != GB_OK ||
+      (st = t.get((nblk + 1) * 4, (void**)&blocks, w)) != GB_OK ||
+      (st = t.get(8, (void**)&total, w)) != GB_OK) {
     dev_free(c, primes);
     dev_free(c, magic);
     return st;
   }
+  auto bail = [&](cudaError_t e, const char* what) {
+    dev_free(c, primes);
+    dev_free(c, magic);
+    return cuda_fail(w, e, what);
+  };
   uint64_t cur = 0, count = 0;
   std::vector<uint32_t> head;
   while (cur < target) {
-    uint64_t next = cur == 0 ? std::min<uint64_t>(target, 5039) : std::min<uint64_t>(target, (cur + 1) * (cur + 1) - 1);
-    if (next > target) next = target;
+    uint64_t next = cur == 0 ? std::min<uint64_t>(target, 5039)
+                             : std::min<uint64_t>(target, (cur + 1) * (cur + 1) - 1);
     const uint64_t nbits = (next - 3) / 2 + 1;
     uint64_t nsieve = kWheelPrimeCount + 1, kcoop = kWheelPrimeCount + 1;
     const uint32_t tile = 1u << 18;
@@ -166,44 +220,268 @@ gb_status ensure_primes(gb_ctx* c, uint64_t limit) {
     unsigned long long tot = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&tot, total, 8, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    if (e != cudaSuccess) {
-      cleanup();
-      dev_free(c, primes);
-      dev_free(c, magic);
-      return cuda_fail(c, e, "prime table build");
-    }
+    if (e != cudaSuccess) return bail(e, "prime table build");
     count = tot;
-    if (count > cap) {
-      cleanup();
-      dev_free(c, primes);
-      dev_free(c, magic);
-      return fail(c, GB_ECUDA, "prime table overflow");
-    }
+    if (count > cap) return bail(cudaErrorInvalidValue, "prime table overflow");
     const uint64_t nh = std::min<uint64_t>(count, 8192);
     head.resize(nh);
     e = cudaMemcpy(head.data(), primes, nh * 4, cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) {
-      cleanup();
-      dev_free(c, primes);
-      dev_free(c, magic);
-      return cuda_fail(c, e, "prime table copy");
-    }
+    if (e != cudaSuccess) return bail(e, "prime table copy");
     cur = next;
   }
-  cleanup();
+  t.release();
   dev_free(c, c->d_primes);
   dev_free(c, c->d_magic);
   c->d_primes = primes;
   c->d_magic = magic;
   c->nprimes = count;
   c->primes_limit = target;
-  // host copy of the small primes (parameter derivation only)
   const uint64_t nh = std::min<uint64_t>(count, pi_upper(kHostPrimeLimit));
-  std::vector<uint32_t> h(nh);
+  std::vector<uint32_t> h(nh);  // host copy of the small primes: parameter derivation only
   GB_CU(cudaMemcpy(h.data(), primes, nh * 4, cudaMemcpyDeviceToHost), "prime table copy");
-  size_t keep = std::upper_bound(h.begin(), h.end(), (uint32_t)kHostPrimeLimit) - h.begin();
-  h.resize(keep);
+  h.resize(std::upper_bound(h.begin(), h.end(), (uint32_t)kHostPrimeLimit) - h.begin());
   c->h_primes.swap(h);
+  const uint64_t ns = (count + kSampleStride - 1) / kSampleStride;
+  std::vector<uint32_t> smp(ns);
+  GB_CU(cudaMemcpy2D(smp.data(), 4, primes, kSampleStride * 4, 4, ns, cudaMemcpyDeviceToHost),
+        "prime table sample");
+  c->h_sample.swap(smp);
+  return GB_OK;
+}
+
+// ---------------------------------------------------------------------------
+gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint64_t limit,
+                     const gb_range_opts* opts, gb_range_result* res, const gb_range_out* out) {
+  if (limit & 1) limit--;
+  if (start < 4) start = 4;
+  if (start & 1) start++;
+  if (start > limit) return fail(w, GB_EINVAL, "START must be less than LIMIT");
+  gb_range_opts o{};
+  if (opts) o = *opts;
+  if (!o.seg_size) o.seg_size = 10000000ull;
+  if (!o.p_small) o.p_small = 1000000ull;
+  if (!o.phase2_limit) o.phase2_limit = GB_PHASE2_LIMIT_DEFAULT;
+  if (o.p_small > GB_P_SMALL_MAX)
+    return fail(w, GB_EINVAL, "P_SMALL must be <= 4000000000 to prevent mathematical overflow.");
+  if (o.phase2_limit > GB_P_SMALL_MAX) return fail(w, GB_EINVAL, "phase2_limit must be <= 4e9");
+  const uint64_t count = (limit - start) / 2 + 1;
+  const uint32_t H = o.halo ? o.halo : 32768u;
+  if (H < 128 || H > (1u << 17) || (H & 63))
+    return fail(w, GB_EINVAL, "halo must be a multiple of 64 in [128, 2^17]");
+  uint32_t NE = o.chunk_evens;
+  if (!NE) {
+    NE = 1u << 19;
+    while (NE > 8192 && NE / 2 >= count) NE >>= 1;
+  }
+  if (NE < 8192 || NE > (1u << 20) || (NE & (NE - 1)))
+    return fail(w, GB_EINVAL, "chunk_evens must be a power of two in [2^13, 2^20]");
+  const uint32_t sc = o.shard_count ? o.shard_count : 1;
+  if (o.shard_index >= sc) return fail(w, GB_EINVAL, "shard_index >= shard_count");
+  const uint64_t nseg = (count + o.seg_size - 1) / o.seg_size;
+  const uint64_t my_segs = nseg > o.shard_index ? (nseg - o.shard_index + sc - 1) / sc : 0;
+  const uint64_t cps = (o.seg_size + NE - 1) / NE;
+  const uint64_t p_lim = std::max(o.p_small, o.phase2_limit);
+  const uint64_t root = isqrt_u64(limit);
+  gb_status st = ensure_primes(c, w, std::max<uint64_t>({p_lim, (uint64_t)H, root + 2}));
+  if (st != GB_OK) return st;
+
+  RangeArgs a{};
+  SearchParams& sp = a.s;
+  a.start = start;
+  a.total_count = count;
+  a.seg_size = o.seg_size;
+  a.shard_index = o.shard_index;
+  a.shard_count = sc;
+  a.chunks_per_seg = cps;
+  a.total_items = my_segs * cps;
+  a.chunk_evens = NE;
+  a.nbw = (H / 2 + NE) / 32 + 2;
+  uint64_t ns = 0, kf = 0, nsv = 0, kc = 0;
+  if ((st = count_le(c, w, std::min<uint64_t>(H - 1, p_lim), &ns)) != GB_OK ||
+      (st = count_le(c, w, o.p_small, &kf)) != GB_OK ||
+      (st = count_le(c, w, root, &nsv)) != GB_OK ||
+      (st = count_le(c, w, (H / 2 + NE) / 64, &kc)) != GB_OK)
+    return st;
+  sp.halo = H;
+  sp.nsearch = (uint32_t)ns;
+  sp.klock = (uint32_t)std::min<uint64_t>(ns, kLockPrimes);
+  sp.kfb = (uint32_t)std::min<uint64_t>(kf, 0xffffffffu);
+  sp.p_lim = p_lim;
+  sp.p_small = o.p_small;
+  sp.primes = c->d_primes;
+  sp.nprimes = c->nprimes;
+  sp.ctr = w.ctr;
+  sp.hist = w.hist;
+  sp.queue = w.queue;
+  sp.queue_cap = w.queue_cap;
+  a.magic = c->d_magic;
+  a.nsieve = (uint32_t)std::max<uint64_t>(nsv, kWheelPrimeCount + 1);
+  a.kcoop = (uint32_t)std::max<uint64_t>(kc, kWheelPrimeCount + 1);
+  a.wheel = c->d_wheel;
+
+  cudaStream_t s = o.stream ? (cudaStream_t)o.stream : c->stream;
+  gb_range_out od{};
+  if (out) od = *out;
+  Temps tmp(c, arena);
+  auto dev_out = [&](void* user, size_t bytes, void** dptr) -> gb_status {
+    *dptr = nullptr;
+    if (!user) return GB_OK;
+    if (o.on_device) {
+      *dptr = user;
+      return GB_OK;
+    }
+    return tmp.get(bytes, dptr, w);
+  };
+  const uint64_t vwords = (count + 31) / 32;
+  void *d_vbits, *d_minp, *d_shist, *d_sfb, *d_sfail;
+  if ((st = dev_out(od.verified_bits, vwords * 4, &d_vbits)) != GB_OK ||
+      (st = dev_out(od.min_p, count * 4, &d_minp)) != GB_OK ||
+      (st = dev_out(od.seg_hist, nseg * GB_HIST_BINS * 8, &d_shist)) != GB_OK ||
+      (st = dev_out(od.seg_fallbacks, nseg * 4, &d_sfb)) != GB_OK ||
+      (st = dev_out(od.seg_failures, nseg * 4, &d_sfail)) != GB_OK)
+    return st;
+  if (od.minp_hist && o.on_device) sp.hist = (unsigned long long*)od.minp_hist;
+  sp.vbits = (uint32_t*)d_vbits;
+  sp.minp = (uint32_t*)d_minp;
+  sp.unit_hist = (unsigned long long*)d_shist;
+  sp.unit_fallbacks = (uint32_t*)d_sfb;
+  sp.unit_failures = (uint32_t*)d_sfail;
+
+  cudaError_t e = cudaSuccess;
+  auto chk = [&](cudaError_t x) {
+    if (e == cudaSuccess && x != cudaSuccess) e = x;
+  };
+  uint32_t last_word = count & 31 ? (1u << (count & 31)) - 1 : 0xffffffffu;
+  chk(cudaEventRecord(w.ev0, s));
+  chk(cudaMemsetAsync(sp.ctr, 0, kCtrCount * 8, s));
+  chk(cudaMemsetAsync(sp.ctr + kCtrFirstFail, 0xff, 8, s));
+  chk(cudaMemsetAsync(sp.hist, 0, GB_HIST_BINS * 8, s));
+  if (sp.vbits) {
+    chk(cudaMemsetAsync(sp.vbits, 0xff, vwords * 4, s));
+    // bits past the last n are zero (pageable source: staged at the call)
+    if (count & 31) chk(cudaMemcpyAsync(sp.vbits + vwords - 1, &last_word, 4, cudaMemcpyHostToDevice, s));
+  }
+  if (sp.minp) chk(cudaMemsetAsync(sp.minp, 0, count * 4, s));
+  if (sp.unit_hist) chk(cudaMemsetAsync(sp.unit_hist, 0, nseg * GB_HIST_BINS * 8, s));
+  if (sp.unit_fallbacks) chk(cudaMemsetAsync(sp.unit_fallbacks, 0, nseg * 4, s));
+  if (sp.unit_failures) chk(cudaMemsetAsync(sp.unit_failures, 0, nseg * 4, s));
+  if (e != cudaSuccess) return cuda_fail(w, e, "range setup");
+  int launches = 0;
+  int bps = range_max_blocks_per_sm(a);
+  if (bps < 1) bps = 1;
+  uint64_t grid = (uint64_t)c->sm_count * bps;
+  if (a.total_items < grid) grid = std::max<uint64_t>(1, a.total_items);
+  if (a.total_items) {
+    chk(cudaEventRecord(w.ek0, s));
+    chk(launch_range(a, (int)grid, s));
+    chk(cudaEventRecord(w.ek1, s));
+    chk(launch_fallback(sp, c->sm_count * 4, s));
+    launches += 2;
+  }
+  chk(cudaEventRecord(w.ev1, s));
+  unsigned long long ctr[kCtrCount];
+  chk(cudaMemcpyAsync(ctr, sp.ctr, sizeof ctr, cudaMemcpyDeviceToHost, s));
+  if (od.minp_hist && !o.on_device)
+    chk(cudaMemcpyAsync(od.minp_hist, sp.hist, GB_HIST_BINS * 8, cudaMemcpyDeviceToHost, s));
+  if (!o.on_device) {
+    if (od.verified_bits) chk(cudaMemcpyAsync(od.verified_bits, sp.vbits, vwords * 4, cudaMemcpyDeviceToHost, s));
+    if (od.min_p) chk(cudaMemcpyAsync(od.min_p, sp.minp, count * 4, cudaMemcpyDeviceToHost, s));
+    if (od.seg_hist) chk(cudaMemcpyAsync(od.seg_hist, sp.unit_hist, nseg * GB_HIST_BINS * 8, cudaMemcpyDeviceToHost, s));
+    if (od.seg_fallbacks) chk(cudaMemcpyAsync(od.seg_fallbacks, sp.unit_fallbacks, nseg * 4, cudaMemcpyDeviceToHost, s));
+    if (od.seg_failures) chk(cudaMemcpyAsync(od.seg_failures, sp.unit_failures, nseg * 4, cudaMemcpyDeviceToHost, s));
+  }
+  chk(cudaStreamSynchronize(s));
+  float ms = 0, kms = 0;
+  if (e == cudaSuccess) {
+    cudaEventElapsedTime(&ms, w.ev0, w.ev1);
+    if (a.total_items) cudaEventElapsedTime(&kms, w.ek0, w.ek1);
+  }
+  if (e != cudaSuccess) return cuda_fail(w, e, "range verification");
+  if (ctr[kCtrQueueOvf]) return fail(w, GB_EOVERFLOW, "Phase-2 queue overflow: raise the halo");
+  if (res) {
+    std::memset(res, 0, sizeof *res);
+    uint64_t checked = 0;
+    for (uint64_t sgi = o.shard_index; sgi < nseg; sgi += sc)
+      checked += std::min<uint64_t>(o.seg_size, count - sgi * o.seg_size);
+    res->checked = checked;
+    res->failures = ctr[kCtrFailures];
+    res->verified = checked - ctr[kCtrFailures];
+    res->phase2_fallbacks = ctr[kCtrFallbacks];
+    res->first_failure_n = ctr[kCtrFailures] ? ctr[kCtrFirstFail] : 0;
+    res->max_minp = ctr[kCtrMaxP];
+    res->num_segments = nseg;
+    res->queued = std::min<uint64_t>(ctr[kCtrQueue], w.queue_cap);
+    res->kernel_launches = launches;
+    res->device_ms = ms;
+    res->kernel_ms = kms;
+  }
+  return GB_OK;
+}
+
+// ---------------------------------------------------------------------------
+gb_status single_impl(gb_ctx* c, Workspace& w, Arena* arena, const uint64_t* n, size_t count,
+                      uint64_t* p_out, uint64_t* q_out, const gb_single_opts* opts,
+                      gb_single_result* res) {
+  if (count && (!n || !p_out || !q_out)) return fail(w, GB_EINVAL, "null buffer");
+  gb_single_opts o{};
+  if (opts) o = *opts;
+  if (!o.p_limit) o.p_limit = GB_PHASE2_LIMIT_DEFAULT;
+  if (o.p_limit > 0xfffffffbull) return fail(w, GB_EINVAL, "p_limit above 2^32");
+  gb_status st = ensure_primes(c, w, o.p_limit);
+  if (st != GB_OK) return st;
+  uint64_t np = 0;
+  if ((st = count_le(c, w, o.p_limit, &np)) != GB_OK) return st;
+  cudaStream_t s = o.stream ? (cudaStream_t)o.stream : c->stream;
+  const uint64_t* dn = n;
+  uint64_t *dp = p_out, *dq = q_out;
+  Temps tmp(c, arena);
+  if (!o.on_device && count) {
+    void* t;
+    if ((st = tmp.get(count * 8 * 3, &t, w)) != GB_OK) return st;
+    dn = (const uint64_t*)t;
+    dp = (uint64_t*)t + count;
+    dq = (uint64_t*)t + 2 * count;
+  }
+  cudaError_t e = cudaSuccess;
+  auto chk = [&](cudaError_t x) {
+    if (e == cudaSuccess && x != cudaSuccess) e = x;
+  };
+  chk(cudaEventRecord(w.ev0, s));
+  if (!o.on_device && count) chk(cudaMemcpyAsync((void*)dn, n, count * 8, cudaMemcpyHostToDevice, s));
+  chk(cudaMemsetAsync(w.ctr, 0, 4 * 8, s));
+  int launches = 0;
+  if (count) {
+    SingleArgs a{};
+    a.n = dn;
+    a.count = count;
+    a.p_out = dp;
+    a.q_out = dq;
+    a.primes = c->d_primes;
+    a.nprimes = np;
+    a.p_lim = o.p_limit;
+    a.ctr = w.ctr;
+    uint64_t grid = (uint64_t)c->sm_count * 6;
+    grid = std::min<uint64_t>(grid, (count + 7) / 8);
+    chk(launch_single(a, (int)std::max<uint64_t>(grid, 1), s));
+    ++launches;
+  }
+  if (!o.on_device && count) {
+    chk(cudaMemcpyAsync(p_out, dp, count * 8, cudaMemcpyDeviceToHost, s));
+    chk(cudaMemcpyAsync(q_out, dq, count * 8, cudaMemcpyDeviceToHost, s));
+  }
+  chk(cudaEventRecord(w.ev1, s));
+  unsigned long long ctr[4] = {0, 0, 0, 0};
+  chk(cudaMemcpyAsync(ctr, w.ctr, sizeof ctr, cudaMemcpyDeviceToHost, s));
+  chk(cudaStreamSynchronize(s));
+  float ms = 0;
+  if (e == cudaSuccess) cudaEventElapsedTime(&ms, w.ev0, w.ev1);
+  if (e != cudaSuccess) return cuda_fail(w, e, "single batch");
+  if (res) {
+    res->found = ctr[1];
+    res->max_p = ctr[2];
+    res->kernel_launches = launches;
+    res->device_ms = ms;
+  }
   return GB_OK;
 }
 
@@ -270,7 +548,7 @@ uint64_t gb_estimate_device_bytes(const gb_config* cfg) {
   // primes + reciprocals, the build bitset and scan blocks, wheel, counters,
   // histogram and the Phase-2 queue
   return np * 12 + want / 16 + (want / 65536 + 1) * 4 + kWheelWords * 4 + kCtrCount * 8 +
-         GB_HIST_BINS * 8 + (8ull << 20);
+         GB_HIST_BINS * 8 + (1ull << 20) * sizeof(QEntry);
 }
 
 gb_status gb_create(int device, const gb_config* cfg, gb_ctx** out) {
@@ -291,25 +569,18 @@ gb_status gb_create(int device, const gb_config* cfg, gb_ctx** out) {
   };
   if (cudaSetDevice(device) != cudaSuccess) return bail(GB_ECUDA);
   cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
-      cudaEventCreate(&c->ev_k0) != cudaSuccess || cudaEventCreate(&c->ev_k1) != cudaSuccess)
-    return bail(GB_ECUDA);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(GB_ECUDA);
   size_t fr = 0, tot = 0;
   cudaMemGetInfo(&fr, &tot);
   c->budget = (cfg && cfg->device_mem_budget) ? cfg->device_mem_budget : (uint64_t)fr;
   if (dev_alloc(c, (void**)&c->d_wheel, kWheelWords * 4) != GB_OK) return bail(GB_ENOMEM);
   if (launch_wheel_init(c->d_wheel, c->stream) != cudaSuccess) return bail(GB_ECUDA);
-  if (dev_alloc(c, (void**)&c->d_ctr, kCtrCount * 8) != GB_OK ||
-      dev_alloc(c, (void**)&c->d_hist, GB_HIST_BINS * 8) != GB_OK)
-    return bail(GB_ENOMEM);
-  c->queue_cap = 1u << 20;
-  if (dev_alloc(c, (void**)&c->d_queue, (size_t)c->queue_cap * sizeof(QEntry)) != GB_OK) return bail(GB_ENOMEM);
+  gb_status st = ws_init(c, c->ws, 1u << 20);
+  if (st != GB_OK) return bail(st);
   uint64_t want = GB_PHASE2_LIMIT_DEFAULT;
   if (cfg && cfg->cand_limit) want = cfg->cand_limit;
   if (cfg && cfg->max_n) want = std::max<uint64_t>(want, isqrt_u64(cfg->max_n) + 2);
-  gb_status st = ensure_primes(c, want);
-  if (st != GB_OK) return bail(st);
+  if ((st = ensure_primes(c, c->ws, want)) != GB_OK) return bail(st);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(GB_ECUDA);
   *out = c;
   return GB_OK;
@@ -322,13 +593,10 @@ void gb_destroy(gb_ctx* c) {
   gb_serve_shutdown(c);
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  ws_free(c, c->ws);
   std::vector<void*> ptrs;
   for (auto& kv : c->allocs) ptrs.push_back(kv.first);
   for (void* p : ptrs) dev_free(c, p);
-  if (c->ev0) cudaEventDestroy(c->ev0);
-  if (c->ev1) cudaEventDestroy(c->ev1);
-  if (c->ev_k0) cudaEventDestroy(c->ev_k0);
-  if (c->ev_k1) cudaEventDestroy(c->ev_k1);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -342,212 +610,53 @@ uint64_t gb_num_segments(uint64_t start, uint64_t limit, uint64_t seg_size) {
   return (count + seg_size - 1) / seg_size;
 }
 
-// ---------------------------------------------------------------------------
+#define GB_PUBLIC(ctx, call)                  \
+  do {                                        \
+    std::lock_guard<std::mutex> lk(ctx->mu);  \
+    cudaSetDevice(ctx->device);               \
+    ctx->ws.err.clear();                      \
+    const gb_status st_ = (call);             \
+    ctx->err = ctx->ws.err;                   \
+    return st_;                               \
+  } while (0)
+
 gb_status gb_verify_range(gb_ctx* c, uint64_t start, uint64_t limit, const gb_range_opts* opts,
                           gb_range_result* res, const gb_range_out* out) {
   if (!c) return GB_EINVAL;
-  std::lock_guard<std::mutex> lk(c->mu);
-  c->err.clear();
-  if (limit & 1) limit--;
-  if (start < 4) start = 4;
-  if (start & 1) start++;
-  if (start > limit) return fail(c, GB_EINVAL, "START must be less than LIMIT");
-  gb_range_opts o{};
-  if (opts) o = *opts;
-  if (!o.seg_size) o.seg_size = 10000000ull;
-  if (!o.p_small) o.p_small = 1000000ull;
-  if (!o.phase2_limit) o.phase2_limit = GB_PHASE2_LIMIT_DEFAULT;
-  if (o.p_small > GB_P_SMALL_MAX)
-    return fail(c, GB_EINVAL, "P_SMALL must be <= 4000000000 to prevent mathematical overflow.");
-  if (o.phase2_limit > GB_P_SMALL_MAX) return fail(c, GB_EINVAL, "phase2_limit must be <= 4e9");
-  const uint64_t count = (limit - start) / 2 + 1;
-  uint32_t H = o.halo ? o.halo : 32768u;
-  if (H < 128 || H > (1u << 17) || (H & 63)) return fail(c, GB_EINVAL, "halo must be a multiple of 64 in [128, 2^17]");
-  uint32_t NE = o.chunk_evens;
-  if (!NE) {
-    NE = 1u << 19;
-    while (NE > 8192 && NE / 2 >= count) NE >>= 1;
-  }
-  if (NE < 8192 || NE > (1u << 20) || (NE & (NE - 1)))
-    return fail(c, GB_EINVAL, "chunk_evens must be a power of two in [2^13, 2^20]");
-  const uint32_t sc = o.shard_count ? o.shard_count : 1;
-  if (o.shard_index >= sc) return fail(c, GB_EINVAL, "shard_index >= shard_count");
-  const uint64_t nseg = (count + o.seg_size - 1) / o.seg_size;
-  const uint64_t my_segs = nseg > o.shard_index ? (nseg - o.shard_index + sc - 1) / sc : 0;
-  const uint64_t cps = (o.seg_size + NE - 1) / NE;
-  const uint64_t p_lim = std::max(o.p_small, o.phase2_limit);
-  const uint64_t root = isqrt_u64(limit);
-  gb_status st = ensure_primes(c, std::max<uint64_t>({p_lim, (uint64_t)H, root + 2}));
-  if (st != GB_OK) return st;
-  cudaSetDevice(c->device);
-
-  RangeArgs a{};
-  SearchParams& sp = a.s;
-  a.start = start;
-  a.total_count = count;
-  a.seg_size = o.seg_size;
-  a.shard_index = o.shard_index;
-  a.shard_count = sc;
-  a.chunks_per_seg = cps;
-  a.total_items = my_segs * cps;
-  a.chunk_evens = NE;
-  a.nbw = (H / 2 + NE) / 32 + 2;
-  uint64_t ns = 0, kf = 0, nsv = 0, kc = 0;
-  if ((st = count_le(c, std::min<uint64_t>(H - 1, p_lim), &ns)) != GB_OK) return st;
-  if ((st = count_le(c, o.p_small, &kf)) != GB_OK) return st;
-  if ((st = count_le(c, root, &nsv)) != GB_OK) return st;
-  if ((st = count_le(c, (H / 2 + NE) / 64, &kc)) != GB_OK) return st;
-  sp.halo = H;
-  sp.nsearch = (uint32_t)ns;
-  sp.klock = (uint32_t)std::min<uint64_t>(ns, kLockPrimes);
-  sp.kfb = (uint32_t)std::min<uint64_t>(kf, 0xffffffffu);
-  sp.p_lim = p_lim;
-  sp.p_small = o.p_small;
-  sp.primes = c->d_primes;
-  sp.nprimes = c->nprimes;
-  sp.ctr = c->d_ctr;
-  sp.hist = c->d_hist;
-  sp.queue = c->d_queue;
-  sp.queue_cap = c->queue_cap;
-  a.magic = c->d_magic;
-  a.nsieve = (uint32_t)std::max<uint64_t>(nsv, kWheelPrimeCount + 1);
-  a.kcoop = (uint32_t)std::max<uint64_t>(kc, kWheelPrimeCount + 1);
-  a.wheel = c->d_wheel;
-
-  cudaStream_t s = o.stream ? (cudaStream_t)o.stream : c->stream;
-  gb_range_out od{};
-  if (out) od = *out;
-  // device buffers for outputs the caller wants on the host
-  std::vector<void*> temps;
-  auto cleanup = [&]() {
-    for (void* p : temps) dev_free(c, p);
-  };
-  auto dev_out = [&](void* user, size_t bytes, void** dptr) -> gb_status {
-    *dptr = nullptr;
-    if (!user) return GB_OK;
-    if (o.on_device) {
-      *dptr = user;
-      return GB_OK;
-    }
-    gb_status r = dev_alloc(c, dptr, bytes);
-    if (r == GB_OK) temps.push_back(*dptr);
-    return r;
-  };
-  const uint64_t vwords = (count + 31) / 32;
-  void *d_vbits, *d_minp, *d_shist, *d_sfb, *d_sfail, *d_hist_user;
-  if ((st = dev_out(od.verified_bits, vwords * 4, &d_vbits)) != GB_OK ||
-      (st = dev_out(od.min_p, count * 4, &d_minp)) != GB_OK ||
-      (st = dev_out(od.seg_hist, nseg * GB_HIST_BINS * 8, &d_shist)) != GB_OK ||
-      (st = dev_out(od.seg_fallbacks, nseg * 4, &d_sfb)) != GB_OK ||
-      (st = dev_out(od.seg_failures, nseg * 4, &d_sfail)) != GB_OK) {
-    cleanup();
-    return st;
-  }
-  d_hist_user = (od.minp_hist && o.on_device) ? (void*)od.minp_hist : nullptr;
-  if (d_hist_user) sp.hist = (unsigned long long*)d_hist_user;
-  sp.vbits = (uint32_t*)d_vbits;
-  sp.minp = (uint32_t*)d_minp;
-  sp.unit_hist = (unsigned long long*)d_shist;
-  sp.unit_fallbacks = (uint32_t*)d_sfb;
-  sp.unit_failures = (uint32_t*)d_sfail;
-
-  cudaError_t e = cudaSuccess;
-  auto chk = [&](cudaError_t x) {
-    if (e == cudaSuccess && x != cudaSuccess) e = x;
-  };
-  chk(cudaEventRecord(c->ev0, s));
-  chk(cudaMemsetAsync(sp.ctr, 0, kCtrCount * 8, s));
-  chk(cudaMemsetAsync(sp.ctr + kCtrFirstFail, 0xff, 8, s));
-  chk(cudaMemsetAsync(sp.hist, 0, GB_HIST_BINS * 8, s));
-  if (sp.vbits) {
-    chk(cudaMemsetAsync(sp.vbits, 0xff, vwords * 4, s));
-    if (count & 31) {  // bits past the last n are zero (pageable source: staged at call)
-      const uint32_t last = (1u << (count & 31)) - 1;
-      chk(cudaMemcpyAsync(sp.vbits + vwords - 1, &last, 4, cudaMemcpyHostToDevice, s));
-    }
-  }
-  if (sp.minp) chk(cudaMemsetAsync(sp.minp, 0, count * 4, s));
-  if (sp.unit_hist) chk(cudaMemsetAsync(sp.unit_hist, 0, nseg * GB_HIST_BINS * 8, s));
-  if (sp.unit_fallbacks) chk(cudaMemsetAsync(sp.unit_fallbacks, 0, nseg * 4, s));
-  if (sp.unit_failures) chk(cudaMemsetAsync(sp.unit_failures, 0, nseg * 4, s));
-  if (e != cudaSuccess) {
-    cleanup();
-    return cuda_fail(c, e, "range setup");
-  }
-  int launches = 0;
-  int bps = range_max_blocks_per_sm(a);
-  if (bps < 1) bps = 1;
-  uint64_t grid = (uint64_t)c->sm_count * bps;
-  if (a.total_items < grid) grid = std::max<uint64_t>(1, a.total_items);
-  if (a.total_items) {
-    chk(cudaEventRecord(c->ev_k0, s));
-    chk(launch_range(a, (int)grid, s));
-    chk(cudaEventRecord(c->ev_k1, s));
-    chk(launch_fallback(sp, c->sm_count * 4, s));
-    launches += 2;
-  }
-  chk(cudaEventRecord(c->ev1, s));
-  unsigned long long ctr[kCtrCount];
-  chk(cudaMemcpyAsync(ctr, sp.ctr, sizeof ctr, cudaMemcpyDeviceToHost, s));
-  if (od.minp_hist && !o.on_device)
-    chk(cudaMemcpyAsync(od.minp_hist, sp.hist, GB_HIST_BINS * 8, cudaMemcpyDeviceToHost, s));
-  if (!o.on_device) {
-    if (od.verified_bits) chk(cudaMemcpyAsync(od.verified_bits, sp.vbits, vwords * 4, cudaMemcpyDeviceToHost, s));
-    if (od.min_p) chk(cudaMemcpyAsync(od.min_p, sp.minp, count * 4, cudaMemcpyDeviceToHost, s));
-    if (od.seg_hist) chk(cudaMemcpyAsync(od.seg_hist, sp.unit_hist, nseg * GB_HIST_BINS * 8, cudaMemcpyDeviceToHost, s));
-    if (od.seg_fallbacks) chk(cudaMemcpyAsync(od.seg_fallbacks, sp.unit_fallbacks, nseg * 4, cudaMemcpyDeviceToHost, s));
-    if (od.seg_failures) chk(cudaMemcpyAsync(od.seg_failures, sp.unit_failures, nseg * 4, cudaMemcpyDeviceToHost, s));
-  }
-  chk(cudaStreamSynchronize(s));
-  float ms = 0, kms = 0;
-  if (e == cudaSuccess) {
-    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-    if (a.total_items) cudaEventElapsedTime(&kms, c->ev_k0, c->ev_k1);
-  }
-  cleanup();
-  if (e != cudaSuccess) return cuda_fail(c, e, "range verification");
-  if (ctr[kCtrQueueOvf]) return fail(c, GB_EOVERFLOW, "Phase-2 queue overflow: raise the halo");
-  if (res) {
-    std::memset(res, 0, sizeof *res);
-    uint64_t checked = 0;
-    for (uint64_t sgi = o.shard_index; sgi < nseg; sgi += sc)
-      checked += std::min<uint64_t>(o.seg_size, count - sgi * o.seg_size);
-    res->checked = checked;
-    res->failures = ctr[kCtrFailures];
-    res->verified = checked - ctr[kCtrFailures];
-    res->phase2_fallbacks = ctr[kCtrFallbacks];
-    res->first_failure_n = ctr[kCtrFailures] ? ctr[kCtrFirstFail] : 0;
-    res->max_minp = ctr[kCtrMaxP];
-    res->num_segments = nseg;
-    res->queued = std::min<uint64_t>(ctr[kCtrQueue], c->queue_cap);
-    res->kernel_launches = launches;
-    res->device_ms = ms;
-    res->kernel_ms = kms;
-  }
-  return GB_OK;
+  GB_PUBLIC(c, range_impl(c, c->ws, nullptr, start, limit, opts, res, out));
 }
 
-// ---------------------------------------------------------------------------
-gb_status gb_sieve_bitset(gb_ctx* c, uint64_t q_lo, uint64_t nbits, uint32_t* words,
-                          int on_device, void* stream) {
-  if (!c || !words || !(q_lo & 1)) return GB_EINVAL;
-  std::lock_guard<std::mutex> lk(c->mu);
-  c->err.clear();
+gb_status gb_check_single_batch(gb_ctx* c, const uint64_t* n, size_t count, uint64_t* p_out,
+                                uint64_t* q_out, const gb_single_opts* opts,
+                                gb_single_result* res) {
+  if (!c) return GB_EINVAL;
+  GB_PUBLIC(c, single_impl(c, c->ws, nullptr, n, count, p_out, q_out, opts, res));
+}
+
+gb_status gb_verify_windows(gb_ctx* c, const gb_window* w, size_t count, const gb_windows_opts* opts,
+                            gb_window_result* res, uint32_t* min_p_concat, gb_windows_summary* sum) {
+  if (!c) return GB_EINVAL;
+  GB_PUBLIC(c, windows_impl(c, c->ws, nullptr, w, count, opts, res, min_p_concat, sum));
+}
+
+static gb_status sieve_bitset_impl(gb_ctx* c, Workspace& w, uint64_t q_lo, uint64_t nbits,
+                                   uint32_t* words, int on_device, void* stream) {
+  if (!words || !(q_lo & 1)) return fail(w, GB_EINVAL, "q_lo must be odd");
   if (nbits == 0) return GB_OK;
   const uint64_t top = q_lo + 2 * (nbits - 1);
-  if (top < q_lo) return fail(c, GB_EINVAL, "window passes 2^64");
+  if (top < q_lo) return fail(w, GB_EINVAL, "window passes 2^64");
   const uint64_t root = isqrt_u64(top);
-  gb_status st = ensure_primes(c, root + 2);
+  gb_status st = ensure_primes(c, w, root + 2);
   if (st != GB_OK) return st;
-  cudaSetDevice(c->device);
   cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  Temps tmp(c, nullptr);
   uint32_t* d = words;
   const uint64_t nwords = (nbits + 31) / 32;
-  if (!on_device && (st = dev_alloc(c, (void**)&d, nwords * 4)) != GB_OK) return st;
+  if (!on_device && (st = tmp.get(nwords * 4, (void**)&d, w)) != GB_OK) return st;
   const uint32_t tile = 1u << 18;
   uint64_t ns = 0, kc = 0;
-  count_le(c, root, &ns);
-  count_le(c, tile / 64, &kc);
+  if ((st = count_le(c, w, root, &ns)) != GB_OK || (st = count_le(c, w, tile / 64, &kc)) != GB_OK)
+    return st;
   SieveArgs a{};
   a.q_lo = q_lo;
   a.nbits = nbits;
@@ -561,131 +670,70 @@ gb_status gb_sieve_bitset(gb_ctx* c, uint64_t q_lo, uint64_t nbits, uint32_t* wo
   cudaError_t e = launch_sieve_bits(a, s);
   if (e == cudaSuccess && !on_device) e = cudaMemcpyAsync(words, d, nwords * 4, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (!on_device) dev_free(c, d);
-  if (e != cudaSuccess) return cuda_fail(c, e, "sieve bitset");
+  if (e != cudaSuccess) return cuda_fail(w, e, "sieve bitset");
+  return GB_OK;
+}
+
+gb_status gb_sieve_bitset(gb_ctx* c, uint64_t q_lo, uint64_t nbits, uint32_t* words, int on_device,
+                          void* stream) {
+  if (!c) return GB_EINVAL;
+  GB_PUBLIC(c, sieve_bitset_impl(c, c->ws, q_lo, nbits, words, on_device, stream));
+}
+
+static gb_status primes_upto_impl(gb_ctx* c, Workspace& w, uint64_t limit, uint32_t* primes,
+                                  uint64_t cap, uint64_t* count) {
+  if (!count) return fail(w, GB_EINVAL, "null count");
+  if (limit > 0xfffffffbull) return fail(w, GB_EINVAL, "limit above the 32-bit prime table");
+  gb_status st = ensure_primes(c, w, std::max<uint64_t>(limit, 2));
+  if (st != GB_OK) return st;
+  uint64_t n = 0;
+  if ((st = count_le(c, w, limit, &n)) != GB_OK) return st;
+  *count = n;
+  if (primes && cap) GB_CU(cudaMemcpy(primes, c->d_primes, std::min(n, cap) * 4, cudaMemcpyDeviceToHost), "primes copy");
   return GB_OK;
 }
 
 gb_status gb_primes_upto(gb_ctx* c, uint64_t limit, uint32_t* primes, uint64_t cap, uint64_t* count) {
-  if (!c || !count) return GB_EINVAL;
-  std::lock_guard<std::mutex> lk(c->mu);
-  c->err.clear();
-  if (limit > 0xfffffffbull) return fail(c, GB_EINVAL, "limit above the 32-bit prime table");
-  gb_status st = ensure_primes(c, std::max<uint64_t>(limit, 2));
-  if (st != GB_OK) return st;
-  uint64_t n = 0;
-  if ((st = count_le(c, limit, &n)) != GB_OK) return st;
-  *count = n;
-  if (primes && cap) {
-    cudaError_t e = cudaMemcpy(primes, c->d_primes, std::min(n, cap) * 4, cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return cuda_fail(c, e, "primes copy");
-  }
-  return GB_OK;
+  if (!c) return GB_EINVAL;
+  GB_PUBLIC(c, primes_upto_impl(c, c->ws, limit, primes, cap, count));
 }
 
-gb_status gb_is_prime_batch(gb_ctx* c, const uint64_t* n, size_t count, uint8_t* out,
-                            int on_device, void* stream) {
-  if (!c || (count && (!n || !out))) return GB_EINVAL;
-  std::lock_guard<std::mutex> lk(c->mu);
-  c->err.clear();
+static gb_status is_prime_impl(gb_ctx* c, Workspace& w, const uint64_t* n, size_t count,
+                               uint8_t* out, int on_device, void* stream) {
+  if (count && (!n || !out)) return fail(w, GB_EINVAL, "null buffer");
   if (!count) return GB_OK;
-  cudaSetDevice(c->device);
   cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
   const uint64_t* dn = n;
   uint8_t* dout = out;
+  Temps tmp(c, nullptr);
   gb_status st;
   if (!on_device) {
-    if ((st = dev_alloc(c, (void**)&dn, count * 8)) != GB_OK) return st;
-    if ((st = dev_alloc(c, (void**)&dout, count)) != GB_OK) {
-      dev_free(c, (void*)dn);
+    if ((st = tmp.get(count * 8, (void**)&dn, w)) != GB_OK || (st = tmp.get(count, (void**)&dout, w)) != GB_OK)
       return st;
-    }
   }
   cudaError_t e = cudaSuccess;
   if (!on_device) e = cudaMemcpyAsync((void*)dn, n, count * 8, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = launch_is_prime(dn, count, dout, s);
   if (e == cudaSuccess && !on_device) e = cudaMemcpyAsync(out, dout, count, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (!on_device) {
-    dev_free(c, (void*)dn);
-    dev_free(c, dout);
-  }
-  if (e != cudaSuccess) return cuda_fail(c, e, "is_prime batch");
+  if (e != cudaSuccess) return cuda_fail(w, e, "is_prime batch");
   return GB_OK;
 }
 
-gb_status gb_check_single_batch(gb_ctx* c, const uint64_t* n, size_t count, uint64_t* p_out,
-                                uint64_t* q_out, const gb_single_opts* opts,
-                                gb_single_result* res) {
-  if (!c || (count && (!n || !p_out || !q_out))) return GB_EINVAL;
-  std::lock_guard<std::mutex> lk(c->mu);
-  c->err.clear();
-  gb_single_opts o{};
-  if (opts) o = *opts;
-  if (!o.p_limit) o.p_limit = GB_PHASE2_LIMIT_DEFAULT;
-  if (o.p_limit > 0xfffffffbull) return fail(c, GB_EINVAL, "p_limit above 2^32");
-  gb_status st = ensure_primes(c, o.p_limit);
-  if (st != GB_OK) return st;
-  uint64_t np = 0;
-  if ((st = count_le(c, o.p_limit, &np)) != GB_OK) return st;
-  cudaSetDevice(c->device);
-  cudaStream_t s = o.stream ? (cudaStream_t)o.stream : c->stream;
-  const uint64_t* dn = n;
-  uint64_t *dp = p_out, *dq = q_out;
-  std::vector<void*> temps;
-  auto cleanup = [&]() {
-    for (void* p : temps) dev_free(c, p);
-  };
-  if (!o.on_device && count) {
-    void* t;
-    if ((st = dev_alloc(c, &t, count * 8 * 3)) != GB_OK) return st;
-    temps.push_back(t);
-    dn = (const uint64_t*)t;
-    dp = (uint64_t*)t + count;
-    dq = (uint64_t*)t + 2 * count;
-  }
-  cudaError_t e = cudaSuccess;
-  auto chk = [&](cudaError_t x) {
-    if (e == cudaSuccess && x != cudaSuccess) e = x;
-  };
-  chk(cudaEventRecord(c->ev0, s));
-  if (!o.on_device && count) chk(cudaMemcpyAsync((void*)dn, n, count * 8, cudaMemcpyHostToDevice, s));
-  chk(cudaMemsetAsync(c->d_ctr, 0, 4 * 8, s));
-  int launches = 0;
-  if (count) {
-    SingleArgs a{};
-    a.n = dn;
-    a.count = count;
-    a.p_out = dp;
-    a.q_out = dq;
-    a.primes = c->d_primes;
-    a.nprimes = np;
-    a.p_lim = o.p_limit;
-    a.ctr = c->d_ctr;
-    uint64_t grid = (uint64_t)c->sm_count * 6;
-    grid = std::min<uint64_t>(grid, (count + 7) / 8);
-    chk(launch_single(a, (int)std::max<uint64_t>(grid, 1), s));
-    ++launches;
-  }
-  if (!o.on_device && count) {
-    chk(cudaMemcpyAsync(p_out, dp, count * 8, cudaMemcpyDeviceToHost, s));
-    chk(cudaMemcpyAsync(q_out, dq, count * 8, cudaMemcpyDeviceToHost, s));
-  }
-  chk(cudaEventRecord(c->ev1, s));
-  unsigned long long ctr[4] = {0, 0, 0, 0};
-  chk(cudaMemcpyAsync(ctr, c->d_ctr, sizeof ctr, cudaMemcpyDeviceToHost, s));
-  chk(cudaStreamSynchronize(s));
-  float ms = 0;
-  if (e == cudaSuccess) cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-  cleanup();
-  if (e != cudaSuccess) return cuda_fail(c, e, "single batch");
-  if (res) {
-    res->found = ctr[1];
-    res->max_p = ctr[2];
-    res->kernel_launches = launches;
-    res->device_ms = ms;
-  }
-  return GB_OK;
+gb_status gb_is_prime_batch(gb_ctx* c, const uint64_t* n, size_t count, uint8_t* out, int on_device,
+                            void* stream) {
+  if (!c) return GB_EINVAL;
+  GB_PUBLIC(c, is_prime_impl(c, c->ws, n, count, out, on_device, stream));
 }
 
 }  // extern "C"
+
+extern "C" gb_status gb_probe_peaks(gb_ctx* c, double* alu_ops_per_s, double* smem_atomics_per_s) {
+  if (!c || !alu_ops_per_s || !smem_atomics_per_s) return GB_EINVAL;
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (run_probe(0, c->sm_count, alu_ops_per_s, c->stream) != cudaSuccess ||
+      run_probe(1, c->sm_count, smem_atomics_per_s, c->stream) != cudaSuccess)
+    return GB_ECUDA;
+  return GB_OK;
+}

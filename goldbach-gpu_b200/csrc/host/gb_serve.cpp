@@ -1,5 +1,416 @@
-// gb_serve.cpp -- serving loop (continuous batching of range and single-n
-// requests).  Filled in with the serving entry points.
+// gb_serve.cpp -- serving loop: continuous batching of single-n and range
+// requests over one context's resident tables.
+//
+// No counterpart in the reference, which answers one query per process
+// (`single_check <n>` re-sieves 1e8 candidates on the CPU for every query,
+// src/single_check.cu:186-198).  Here:
+//   * lane 0 (single): single n and short ranges, expanded n by n, through
+//     the single-n kernel plus a per-request reduction;
+//   * lane 1 (range): longer ranges through the windows pipeline.
+// Each lane is a host thread with its own CUDA stream, workspace and device
+// arena reserved at start, so the two lanes' batches overlap on the GPU and
+// nothing is allocated or freed while they run.  When a lane's batch
+// completes it immediately takes every request waiting for it (arrival
+// order, up to its batch size and arena), so requests that arrive while the
+// GPU is busy are admitted as soon as a lane and memory free up.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <thread>
+#include <unordered_map>
+
 #include "gb_ctx.h"
 
-extern "C" void gb_serve_shutdown(gb_ctx* ctx) { (void)ctx; }
+using namespace gb;
+
+namespace {
+
+struct Pending {
+  uint64_t ticket;
+  gb_request r;
+};
+
+struct Lane {
+  Workspace ws;
+  Arena arena;
+  void* arena_mem = nullptr;
+  cudaStream_t stream = nullptr;
+  std::thread th;
+  uint64_t batches = 0;
+};
+
+uint64_t now_ns() {
+  return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+             std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+constexpr uint32_t kSingleReqCap = 1u << 16;  // requests per single-lane batch
+
+}  // namespace
+
+struct gb_server {
+  gb_ctx* c = nullptr;
+  gb_serve_opts o{};
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<Pending> q[2];
+  std::unordered_map<uint64_t, gb_response> done;
+  uint64_t next_ticket = 1;
+  bool stop = false;
+  Lane lane[2];
+  // single-lane pinned staging
+  uint64_t *h_n = nullptr, *h_p = nullptr, *h_off = nullptr;
+  unsigned long long* h_agg = nullptr;
+  // stats
+  std::vector<double> lat;
+  uint64_t submitted = 0, completed = 0, rejected = 0, t0 = 0;
+};
+
+namespace {
+
+// bytes the range lane's windows call takes from its arena for a batch
+uint64_t range_bytes(const gb_request& r) {
+  const uint64_t wbits = ((32768 / 2 + r.count + 64 + 128) + 127) / 128 * 128;
+  return wbits / 8 + 96;
+}
+
+void finish(gb_server* S, const Pending& p, gb_response& resp, uint64_t t_done) {
+  const uint64_t arr = p.r.arrival_ns;
+  resp.latency_us = t_done > arr ? (t_done - arr) / 1e3 : 0.0;
+  std::lock_guard<std::mutex> lk(S->mu);
+  S->done[p.ticket] = resp;
+  S->completed++;
+  if (resp.status == GB_OK) S->lat.push_back(resp.latency_us);
+  S->cv_done.notify_all();
+}
+
+void single_lane(gb_server* S) {
+  Lane& L = S->lane[0];
+  gb_ctx* c = S->c;
+  const uint32_t cap = S->o.max_single_batch;
+  // fixed device layout in the lane arena
+  uint64_t* d_n = (uint64_t*)L.arena.take((size_t)cap * 8);
+  uint64_t* d_p = (uint64_t*)L.arena.take((size_t)cap * 8);
+  uint64_t* d_q = (uint64_t*)L.arena.take((size_t)cap * 8);
+  uint64_t* d_off = (uint64_t*)L.arena.take((size_t)(kSingleReqCap + 1) * 8);
+  unsigned long long* d_agg = (unsigned long long*)L.arena.take((size_t)kSingleReqCap * 32);
+  uint64_t np = 0;
+  count_le(c, L.ws, GB_PHASE2_LIMIT_DEFAULT, &np);
+  std::vector<Pending> take;
+  for (;;) {
+    take.clear();
+    uint64_t total = 0;
+    {
+      std::unique_lock<std::mutex> lk(S->mu);
+      S->cv_work.wait(lk, [&] { return S->stop || !S->q[0].empty(); });
+      if (S->q[0].empty()) break;  // stop requested and drained
+      while (!S->q[0].empty() && take.size() < kSingleReqCap) {
+        const Pending& f = S->q[0].front();
+        const uint64_t w = f.r.kind == GB_REQ_SINGLE ? 1 : f.r.count;
+        if (total + w > cap) break;
+        take.push_back(f);
+        total += w;
+        S->q[0].pop_front();
+      }
+    }
+    uint64_t pos = 0;
+    for (size_t i = 0; i < take.size(); ++i) {
+      S->h_off[i] = pos;
+      const gb_request& r = take[i].r;
+      if (r.kind == GB_REQ_SINGLE) S->h_n[pos++] = r.a;
+      else
+        for (uint64_t j = 0; j < r.count; ++j) S->h_n[pos++] = r.a + 2 * j;
+    }
+    S->h_off[take.size()] = pos;
+    cudaError_t e = cudaSuccess;
+    auto chk = [&](cudaError_t x) {
+      if (e == cudaSuccess && x != cudaSuccess) e = x;
+    };
+    chk(cudaMemcpyAsync(d_n, S->h_n, pos * 8, cudaMemcpyHostToDevice, L.stream));
+    chk(cudaMemcpyAsync(d_off, S->h_off, (take.size() + 1) * 8, cudaMemcpyHostToDevice, L.stream));
+    chk(cudaMemsetAsync(L.ws.ctr, 0, 4 * 8, L.stream));
+    SingleArgs a{};
+    a.n = d_n;
+    a.count = pos;
+    a.p_out = d_p;
+    a.q_out = d_q;
+    a.primes = c->d_primes;
+    a.nprimes = np;
+    a.p_lim = GB_PHASE2_LIMIT_DEFAULT;
+    a.ctr = L.ws.ctr;
+    const uint64_t grid = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)c->sm_count * 6, (pos + 7) / 8));
+    chk(launch_single(a, (int)grid, L.stream));
+    chk(launch_segment_reduce(d_p, d_off, (uint32_t)take.size(), d_agg, L.stream));
+    chk(cudaMemcpyAsync(S->h_p, d_p, pos * 8, cudaMemcpyDeviceToHost, L.stream));
+    chk(cudaMemcpyAsync(S->h_agg, d_agg, take.size() * 32, cudaMemcpyDeviceToHost, L.stream));
+    chk(cudaStreamSynchronize(L.stream));
+    const uint64_t t_done = now_ns();
+    const uint32_t batch = (uint32_t)L.batches++;
+    for (size_t i = 0; i < take.size(); ++i) {
+      gb_response resp{};
+      resp.kind = take[i].r.kind;
+      resp.lane = 0;
+      resp.batch = batch;
+      resp.status = e == cudaSuccess ? GB_OK : GB_ECUDA;
+      if (e == cudaSuccess) {
+        if (resp.kind == GB_REQ_SINGLE) {
+          resp.p = S->h_p[S->h_off[i]];
+          resp.q = resp.p ? take[i].r.a - resp.p : 0;
+        }
+        resp.verified = S->h_agg[4 * i];
+        resp.failures = S->h_agg[4 * i + 1];
+        resp.max_minp = S->h_agg[4 * i + 2];
+        resp.minp_sum = S->h_agg[4 * i + 3];
+      }
+      finish(S, take[i], resp, t_done);
+    }
+  }
+}
+
+void range_lane(gb_server* S) {
+  Lane& L = S->lane[1];
+  gb_ctx* c = S->c;
+  std::vector<Pending> take;
+  std::vector<gb_window> win;
+  std::vector<gb_window_result> res;
+  for (;;) {
+    take.clear();
+    {
+      std::unique_lock<std::mutex> lk(S->mu);
+      S->cv_work.wait(lk, [&] { return S->stop || !S->q[1].empty(); });
+      if (S->q[1].empty()) break;
+      uint64_t bytes = 64 << 10;
+      while (!S->q[1].empty() && take.size() < S->o.max_range_batch) {
+        const Pending& f = S->q[1].front();
+        const uint64_t b = range_bytes(f.r);
+        if (!take.empty() && bytes + b > L.arena.cap) break;
+        take.push_back(f);
+        bytes += b;
+        S->q[1].pop_front();
+      }
+    }
+    win.resize(take.size());
+    res.assign(take.size(), gb_window_result{});
+    for (size_t i = 0; i < take.size(); ++i) win[i] = gb_window{take[i].r.a, take[i].r.count};
+    gb_windows_opts o{};
+    o.mode = GB_WINDOWS_PERSISTENT;
+    o.stream = L.stream;
+    gb_windows_summary sum{};
+    L.arena.used = 0;
+    const gb_status st = windows_impl(c, L.ws, &L.arena, win.data(), win.size(), &o, res.data(),
+                                      nullptr, &sum);
+    L.arena.used = 0;
+    const uint64_t t_done = now_ns();
+    const uint32_t batch = (uint32_t)L.batches++;
+    for (size_t i = 0; i < take.size(); ++i) {
+      gb_response resp{};
+      resp.kind = GB_REQ_RANGE;
+      resp.lane = 1;
+      resp.batch = batch;
+      resp.status = st;
+      if (st == GB_OK) {
+        resp.verified = res[i].verified;
+        resp.failures = res[i].failures;
+        resp.max_minp = res[i].max_minp;
+        resp.minp_sum = res[i].minp_sum;
+      }
+      finish(S, take[i], resp, t_done);
+    }
+  }
+}
+
+void free_server(gb_server* S) {
+  gb_ctx* c = S->c;
+  for (Lane& L : S->lane) {
+    if (L.stream) {
+      cudaStreamSynchronize(L.stream);
+      cudaStreamDestroy(L.stream);
+    }
+    ws_free(c, L.ws);
+    dev_free(c, L.arena_mem);
+  }
+  if (S->h_n) cudaFreeHost(S->h_n);
+  if (S->h_p) cudaFreeHost(S->h_p);
+  if (S->h_off) cudaFreeHost(S->h_off);
+  if (S->h_agg) cudaFreeHost(S->h_agg);
+  delete S;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint64_t gb_now_ns(void) { return now_ns(); }
+
+gb_status gb_serve_start(gb_ctx* c, const gb_serve_opts* opts) {
+  if (!c) return GB_EINVAL;
+  std::lock_guard<std::mutex> lk(c->mu);
+  if (c->server) return GB_EINVAL;
+  cudaSetDevice(c->device);
+  gb_server* S = new gb_server();
+  S->c = c;
+  if (opts) S->o = *opts;
+  if (!S->o.max_n) S->o.max_n = ~0ull;
+  if (!S->o.max_single_batch) S->o.max_single_batch = 1u << 18;
+  if (!S->o.max_range_batch) S->o.max_range_batch = 4096;
+  if (!S->o.range_arena_bytes) S->o.range_arena_bytes = 4ull << 30;
+  if (!S->o.small_range) S->o.small_range = 1u << 15;
+  if (S->o.small_range > S->o.max_single_batch) S->o.small_range = S->o.max_single_batch;
+  // resident tables for every n served: sieving primes to sqrt(max_n) and
+  // the candidate primes; frozen while the lanes run
+  gb_status st = ensure_primes(c, c->ws, std::max<uint64_t>(isqrt_u64(S->o.max_n) + 2,
+                                                            GB_PHASE2_LIMIT_DEFAULT));
+  auto bail = [&](gb_status x) {
+    c->err = c->ws.err;
+    free_server(S);
+    return x;
+  };
+  if (st != GB_OK) return bail(st);
+  const uint64_t cap = S->o.max_single_batch;
+  const uint64_t single_bytes = cap * 24 + (kSingleReqCap + 1) * 8 + kSingleReqCap * 32 + 4096;
+  const uint64_t arena_bytes[2] = {single_bytes, S->o.range_arena_bytes};
+  for (int i = 0; i < 2; ++i) {
+    Lane& L = S->lane[i];
+    if ((st = ws_init(c, L.ws, 1u << 16)) != GB_OK) return bail(st);
+    if ((st = dev_alloc(c, &L.arena_mem, arena_bytes[i], &c->ws.err)) != GB_OK) return bail(st);
+    L.arena.base = (char*)L.arena_mem;
+    L.arena.cap = arena_bytes[i];
+    if (cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking) != cudaSuccess) return bail(GB_ECUDA);
+  }
+  if (cudaHostAlloc((void**)&S->h_n, cap * 8, cudaHostAllocDefault) != cudaSuccess ||
+      cudaHostAlloc((void**)&S->h_p, cap * 8, cudaHostAllocDefault) != cudaSuccess ||
+      cudaHostAlloc((void**)&S->h_off, (kSingleReqCap + 1) * 8, cudaHostAllocDefault) != cudaSuccess ||
+      cudaHostAlloc((void**)&S->h_agg, kSingleReqCap * 32, cudaHostAllocDefault) != cudaSuccess)
+    return bail(GB_ENOMEM);
+  S->t0 = now_ns();
+  c->server = S;
+  S->lane[0].th = std::thread([S] {
+    cudaSetDevice(S->c->device);
+    single_lane(S);
+  });
+  S->lane[1].th = std::thread([S] {
+    cudaSetDevice(S->c->device);
+    range_lane(S);
+  });
+  return GB_OK;
+}
+
+gb_status gb_submit(gb_ctx* c, const gb_request* reqs, size_t count, uint64_t* tickets) {
+  if (!c || (count && (!reqs || !tickets))) return GB_EINVAL;
+  gb_server* S = c->server;
+  if (!S) return GB_EINVAL;
+  const uint64_t t = now_ns();
+  std::lock_guard<std::mutex> lk(S->mu);
+  if (S->stop) return GB_ECANCELED;
+  for (size_t i = 0; i < count; ++i) {
+    Pending p{S->next_ticket++, reqs[i]};
+    if (!p.r.arrival_ns) p.r.arrival_ns = t;
+    tickets[i] = p.ticket;
+    S->submitted++;
+    const gb_request& r = p.r;
+    bool ok = r.a >= 4 && !(r.a & 1) && r.a <= S->o.max_n;
+    if (r.kind == GB_REQ_RANGE) {
+      const uint64_t last = r.a + 2 * (r.count - 1);
+      ok = ok && r.count >= 1 && r.count <= (1ull << 40) && last >= r.a && last <= S->o.max_n;
+    } else if (r.kind != GB_REQ_SINGLE) {
+      ok = false;
+    }
+    gb_status bad = ok ? GB_OK : GB_EINVAL;
+    if (ok && r.kind == GB_REQ_RANGE && r.count > S->o.small_range &&
+        range_bytes(r) + (64 << 10) > S->lane[1].arena.cap)
+      bad = GB_ENOMEM;  // would never fit the range lane's memory
+    if (bad != GB_OK) {
+      gb_response resp{};
+      resp.status = bad;
+      resp.kind = r.kind;
+      S->done[p.ticket] = resp;
+      S->completed++;
+      S->rejected++;
+      continue;
+    }
+    const int ln = (r.kind == GB_REQ_SINGLE || r.count <= S->o.small_range) ? 0 : 1;
+    S->q[ln].push_back(p);
+  }
+  S->cv_work.notify_all();
+  return GB_OK;
+}
+
+gb_status gb_poll(gb_ctx* c, uint64_t ticket, gb_response* out) {
+  if (!c || !c->server || !out) return GB_EINVAL;
+  gb_server* S = c->server;
+  std::lock_guard<std::mutex> lk(S->mu);
+  auto it = S->done.find(ticket);
+  if (it == S->done.end()) return ticket && ticket < S->next_ticket ? GB_EAGAIN : GB_EINVAL;
+  *out = it->second;
+  S->done.erase(it);
+  return GB_OK;
+}
+
+gb_status gb_wait(gb_ctx* c, uint64_t ticket, gb_response* out, uint64_t timeout_ms) {
+  if (!c || !c->server || !out) return GB_EINVAL;
+  gb_server* S = c->server;
+  std::unique_lock<std::mutex> lk(S->mu);
+  const bool got = S->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] {
+    return S->done.count(ticket) != 0;
+  });
+  if (!got) return GB_ETIMEOUT;
+  *out = S->done[ticket];
+  S->done.erase(ticket);
+  return GB_OK;
+}
+
+gb_status gb_serve_stats_get(gb_ctx* c, gb_serve_stats* out, int reset) {
+  if (!c || !c->server || !out) return GB_EINVAL;
+  gb_server* S = c->server;
+  std::lock_guard<std::mutex> lk(S->mu);
+  std::memset(out, 0, sizeof *out);
+  out->submitted = S->submitted;
+  out->completed = S->completed;
+  out->pending = S->q[0].size() + S->q[1].size();
+  out->rejected = S->rejected;
+  out->batches_single = S->lane[0].batches;
+  out->batches_range = S->lane[1].batches;
+  out->elapsed_s = (now_ns() - S->t0) / 1e9;
+  if (!S->lat.empty()) {
+    std::vector<double> v = S->lat;
+    std::sort(v.begin(), v.end());
+    auto pct = [&](double f) { return v[std::min<size_t>(v.size() - 1, (size_t)(f * (v.size() - 1) + 0.5))]; };
+    out->p50_us = pct(0.50);
+    out->p99_us = pct(0.99);
+    out->max_us = v.back();
+    double s = 0;
+    for (double x : v) s += x;
+    out->mean_us = s / v.size();
+    out->completed_per_s = v.size() / std::max(out->elapsed_s, 1e-9);
+  }
+  if (reset) {
+    S->lat.clear();
+    S->t0 = now_ns();
+  }
+  return GB_OK;
+}
+
+gb_status gb_serve_stop(gb_ctx* c) {
+  if (!c || !c->server) return GB_EINVAL;
+  gb_server* S = c->server;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->stop = true;
+  }
+  S->cv_work.notify_all();
+  for (Lane& L : S->lane)
+    if (L.th.joinable()) L.th.join();
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->server = nullptr;
+  free_server(S);
+  return GB_OK;
+}
+
+void gb_serve_shutdown(gb_ctx* c) {
+  if (c && c->server) gb_serve_stop(c);
+}
+
+}  // extern "C"

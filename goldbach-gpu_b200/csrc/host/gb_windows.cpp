@@ -18,45 +18,41 @@ constexpr uint32_t kWinTileBits = 1u << 18;
 constexpr uint64_t kWinSmallPrimeBound = 1ull << 17;  // tile sieve marks primes below this
 }  // namespace gb
 
-using namespace gb;
+namespace gb {
 
-extern "C" gb_status gb_verify_windows(gb_ctx* c, const gb_window* w, size_t count,
-                                       const gb_windows_opts* opts, gb_window_result* res,
-                                       uint32_t* min_p_concat, gb_windows_summary* sum) {
-  if (!c || (count && !w)) return GB_EINVAL;
-  std::lock_guard<std::mutex> lk(c->mu);
-  c->err.clear();
+gb_status windows_impl(gb_ctx* c, Workspace& ws, Arena* arena, const gb_window* w, size_t count,
+                       const gb_windows_opts* opts, gb_window_result* res, uint32_t* min_p_concat,
+                       gb_windows_summary* sum) {
+  if (count && !w) return fail(ws, GB_EINVAL, "null windows");
   gb_windows_opts o{};
   if (opts) o = *opts;
   if (o.mode != GB_WINDOWS_PERSISTENT && o.mode != GB_WINDOWS_PLAIN)
-    return fail(c, GB_EINVAL, "unknown windows mode");
-  if (o.on_device) return fail(c, GB_EINVAL, "windows: on_device outputs are not supported");
+    return fail(ws, GB_EINVAL, "unknown windows mode");
+  if (o.on_device) return fail(ws, GB_EINVAL, "windows: on_device outputs are not supported");
   if (count == 0) {
     if (sum) std::memset(sum, 0, sizeof *sum);
     return GB_OK;
   }
-  if (count > 0xffffffffull) return fail(c, GB_EINVAL, "too many windows");
+  if (count > 0xffffffffull) return fail(ws, GB_EINVAL, "too many windows");
   const uint32_t H = o.halo ? o.halo : 32768u;
-  if (H < 128 || H > (1u << 17) || (H & 63)) return fail(c, GB_EINVAL, "halo must be a multiple of 64 in [128, 2^17]");
+  if (H < 128 || H > (1u << 17) || (H & 63)) return fail(ws, GB_EINVAL, "halo must be a multiple of 64 in [128, 2^17]");
   const uint32_t NE = o.chunk_evens ? o.chunk_evens : (1u << 19);
   if (NE < 8192 || NE > (1u << 20) || (NE & (NE - 1)))
-    return fail(c, GB_EINVAL, "chunk_evens must be a power of two in [2^13, 2^20]");
+    return fail(ws, GB_EINVAL, "chunk_evens must be a power of two in [2^13, 2^20]");
   const uint64_t p_lim = o.phase2_limit ? o.phase2_limit : GB_PHASE2_LIMIT_DEFAULT;
-  if (p_lim > GB_P_SMALL_MAX) return fail(c, GB_EINVAL, "phase2_limit must be <= 4e9");
+  if (p_lim > GB_P_SMALL_MAX) return fail(ws, GB_EINVAL, "phase2_limit must be <= 4e9");
   uint64_t total_n = 0, q_max = 0;
   for (size_t i = 0; i < count; ++i) {
     if (w[i].start < 4 || (w[i].start & 1) || w[i].count == 0)
-      return fail(c, GB_EINVAL, "window start must be even and >= 4, count >= 1");
+      return fail(ws, GB_EINVAL, "window start must be even and >= 4, count >= 1");
     const uint64_t last = w[i].start + 2 * (w[i].count - 1);
-    if (w[i].count > (1ull << 40) || last < w[i].start) return fail(c, GB_EINVAL, "window passes 2^64");
+    if (w[i].count > (1ull << 40) || last < w[i].start) return fail(ws, GB_EINVAL, "window passes 2^64");
     q_max = std::max(q_max, last);
     total_n += w[i].count;
   }
   const uint64_t root = isqrt_u64(q_max);
-  gb_status st = ensure_primes(c, std::max<uint64_t>({p_lim, (uint64_t)H, root + 2, kWinSmallPrimeBound}));
+  gb_status st = ensure_primes(c, ws, std::max<uint64_t>({p_lim, (uint64_t)H, root + 2, kWinSmallPrimeBound}));
   if (st != GB_OK) return st;
-  cudaSetDevice(c->device);
-
   // descriptors, sorted by top q so the large-prime pass visits a suffix
   std::vector<uint32_t> order(count);
   std::iota(order.begin(), order.end(), 0u);
@@ -77,43 +73,31 @@ extern "C" gb_status gb_verify_windows(gb_ctx* c, const gb_window* w, size_t cou
     d.wbase = words;
     d.wbits = ((H / 2 + d.count + 64 + 128) + 127) / 128 * 128;  // slack for 16-byte loads
     d.q_top = d.start + 2 * (d.count - 1);
-    uint64_t nsv = 0;
-    if ((st = count_le(c, isqrt_u64(d.q_top), &nsv)) != GB_OK) return st;
-    d.nsieve = (uint32_t)std::max<uint64_t>(nsv, kWheelPrimeCount + 1);
+    d.nsieve = 0;  // set on the device (launch_win_nsieve)
     d.orig = i;
     words += d.wbits / 32;
     tile_off[r + 1] = tile_off[r] + (d.wbits + kWinTileBits - 1) / kWinTileBits;
     chunk_off[r + 1] = chunk_off[r] + (d.count + NE - 1) / NE;
   }
   uint64_t ns = 0, kf = 0, nsmall = 0, nlarge = 0, kc = 0;
-  if ((st = count_le(c, std::min<uint64_t>(H - 1, p_lim), &ns)) != GB_OK ||
-      (st = count_le(c, p_lim, &kf)) != GB_OK ||
-      (st = count_le(c, kWinSmallPrimeBound, &nsmall)) != GB_OK ||
-      (st = count_le(c, root, &nlarge)) != GB_OK ||
-      (st = count_le(c, kWinTileBits / 64, &kc)) != GB_OK)
+  if ((st = count_le(c, ws, std::min<uint64_t>(H - 1, p_lim), &ns)) != GB_OK ||
+      (st = count_le(c, ws, p_lim, &kf)) != GB_OK ||
+      (st = count_le(c, ws, kWinSmallPrimeBound, &nsmall)) != GB_OK ||
+      (st = count_le(c, ws, root, &nlarge)) != GB_OK ||
+      (st = count_le(c, ws, kWinTileBits / 64, &kc)) != GB_OK)
     return st;
 
-  std::vector<void*> temps;
-  auto cleanup = [&]() {
-    for (void* p : temps) dev_free(c, p);
-  };
-  auto alloc = [&](size_t bytes, void** p) -> gb_status {
-    gb_status r = dev_alloc(c, p, bytes);
-    if (r == GB_OK) temps.push_back(*p);
-    return r;
-  };
+  Temps tmp(c, arena);
   void *d_desc, *d_toff, *d_coff, *d_bits, *d_fail, *d_maxp, *d_psum, *d_minp = nullptr;
-  if ((st = alloc(count * sizeof(WinDesc), &d_desc)) != GB_OK ||
-      (st = alloc((count + 1) * 8, &d_toff)) != GB_OK ||
-      (st = alloc((count + 1) * 8, &d_coff)) != GB_OK ||
-      (st = alloc(words * 4, &d_bits)) != GB_OK ||
-      (st = alloc(count * 4, &d_fail)) != GB_OK ||
-      (st = alloc(count * 8, &d_maxp)) != GB_OK ||
-      (st = alloc(count * 8, &d_psum)) != GB_OK ||
-      (min_p_concat && (st = alloc(total_n * 4, &d_minp)) != GB_OK)) {
-    cleanup();
+  if ((st = tmp.get(count * sizeof(WinDesc), &d_desc, ws)) != GB_OK ||
+      (st = tmp.get((count + 1) * 8, &d_toff, ws)) != GB_OK ||
+      (st = tmp.get((count + 1) * 8, &d_coff, ws)) != GB_OK ||
+      (st = tmp.get(words * 4, &d_bits, ws)) != GB_OK ||
+      (st = tmp.get(count * 4, &d_fail, ws)) != GB_OK ||
+      (st = tmp.get(count * 8, &d_maxp, ws)) != GB_OK ||
+      (st = tmp.get(count * 8, &d_psum, ws)) != GB_OK ||
+      (min_p_concat && (st = tmp.get(total_n * 4, &d_minp, ws)) != GB_OK))
     return st;
-  }
   WindowsArgs a{};
   SearchParams& sp = a.s;
   sp.halo = H;
@@ -124,13 +108,13 @@ extern "C" gb_status gb_verify_windows(gb_ctx* c, const gb_window* w, size_t cou
   sp.p_small = p_lim;
   sp.primes = c->d_primes;
   sp.nprimes = c->nprimes;
-  sp.ctr = c->d_ctr;
+  sp.ctr = ws.ctr;
   sp.unit_failures = (uint32_t*)d_fail;
   sp.unit_maxp = (unsigned long long*)d_maxp;
   sp.unit_psum = (unsigned long long*)d_psum;
   sp.minp = (uint32_t*)d_minp;
-  sp.queue = c->d_queue;
-  sp.queue_cap = c->queue_cap;
+  sp.queue = ws.queue;
+  sp.queue_cap = ws.queue_cap;
   a.win = (const WinDesc*)d_desc;
   a.nwin = (uint32_t)count;
   a.tile_off = (const uint64_t*)d_toff;
@@ -153,6 +137,7 @@ extern "C" gb_status gb_verify_windows(gb_ctx* c, const gb_window* w, size_t cou
     if (e == cudaSuccess && x != cudaSuccess) e = x;
   };
   chk(cudaMemcpyAsync(d_desc, desc.data(), count * sizeof(WinDesc), cudaMemcpyHostToDevice, s));
+  chk(launch_win_nsieve((WinDesc*)d_desc, (uint32_t)count, c->d_primes, c->nprimes, s));
   chk(cudaMemcpyAsync(d_toff, tile_off.data(), (count + 1) * 8, cudaMemcpyHostToDevice, s));
   chk(cudaMemcpyAsync(d_coff, chunk_off.data(), (count + 1) * 8, cudaMemcpyHostToDevice, s));
   chk(cudaMemsetAsync(d_fail, 0, count * 4, s));
@@ -164,7 +149,7 @@ extern "C" gb_status gb_verify_windows(gb_ctx* c, const gb_window* w, size_t cou
   chk(cudaStreamSynchronize(s));  // host vectors above are pageable and local
   int launches = 0;
   const int sm = c->sm_count;
-  chk(cudaEventRecord(c->ev0, s));
+  chk(cudaEventRecord(ws.ev0, s));
   if (o.mode == GB_WINDOWS_PERSISTENT) {
     const uint64_t np = a.nlarge - a.nsmall;
     const int gl = (int)std::min<uint64_t>((np + 255) / 256, (uint64_t)sm * 16);
@@ -172,13 +157,11 @@ extern "C" gb_status gb_verify_windows(gb_ctx* c, const gb_window* w, size_t cou
     chk(launch_fallback(sp, sm * 4, s));
     ++launches;
   } else {
+    const uint64_t np = a.nlarge - a.nsmall;
+    const int gl = (int)std::min<uint64_t>((np + 255) / 256, (uint64_t)sm * 16);
     for (uint32_t r = 0; r < count && e == cudaSuccess; ++r) {
       const uint64_t nt = tile_off[r + 1] - tile_off[r];
       const uint64_t nc = chunk_off[r + 1] - chunk_off[r];
-      uint64_t np = 0;
-      count_le(c, isqrt_u64(desc[r].q_top), &np);
-      np = np > a.nsmall ? np - a.nsmall : 0;
-      const int gl = (int)std::min<uint64_t>((np + 255) / 256, (uint64_t)sm * 16);
       chk(cudaMemsetAsync(sp.ctr + kCtrQueue, 0, 8, s));
       chk(launch_window_stages(a, r, (int)std::min<uint64_t>(nt, sm * 3), gl,
                                (int)std::min<uint64_t>(nc, sm * 2), s, &launches));
@@ -186,7 +169,7 @@ extern "C" gb_status gb_verify_windows(gb_ctx* c, const gb_window* w, size_t cou
       ++launches;
     }
   }
-  chk(cudaEventRecord(c->ev1, s));
+  chk(cudaEventRecord(ws.ev1, s));
   std::vector<uint32_t> fails(count);
   std::vector<uint64_t> maxp(count), psum(count);
   unsigned long long ctr[kCtrCount];
@@ -197,10 +180,9 @@ extern "C" gb_status gb_verify_windows(gb_ctx* c, const gb_window* w, size_t cou
   if (d_minp) chk(cudaMemcpyAsync(min_p_concat, d_minp, total_n * 4, cudaMemcpyDeviceToHost, s));
   chk(cudaStreamSynchronize(s));
   float ms = 0;
-  if (e == cudaSuccess) cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-  cleanup();
-  if (e != cudaSuccess) return cuda_fail(c, e, "windows");
-  if (ctr[kCtrQueueOvf]) return fail(c, GB_EOVERFLOW, "Phase-2 queue overflow: raise the halo");
+  if (e == cudaSuccess) cudaEventElapsedTime(&ms, ws.ev0, ws.ev1);
+  if (e != cudaSuccess) return cuda_fail(ws, e, "windows");
+  if (ctr[kCtrQueueOvf]) return fail(ws, GB_EOVERFLOW, "Phase-2 queue overflow: raise the halo");
   if (res) {
     for (size_t i = 0; i < count; ++i) {
       res[i].failures = fails[i];
@@ -217,3 +199,5 @@ extern "C" gb_status gb_verify_windows(gb_ctx* c, const gb_window* w, size_t cou
   }
   return GB_OK;
 }
+
+}  // namespace gb

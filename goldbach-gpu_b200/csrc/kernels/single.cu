@@ -151,6 +151,46 @@ cudaError_t launch_single(const SingleArgs& a, int grid, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// Per-request totals of a single-lane batch: request r owns the n of
+// [off[r], off[r+1]); agg[4r..4r+3] = verified, failures, max p, sum of p.
+__global__ void segment_reduce_kernel(const uint64_t* p, const uint64_t* off, uint32_t nreq,
+                                      unsigned long long* agg) {
+  const uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= nreq) return;
+  unsigned long long v = 0, f = 0, mx = 0, sum = 0;
+  for (uint64_t i = off[r] + lane; i < off[r + 1]; i += 32) {
+    const uint64_t x = p[i];
+    if (x) {
+      ++v;
+      sum += x;
+      if (x > mx) mx = x;
+    } else {
+      ++f;
+    }
+  }
+  for (int o = 16; o; o >>= 1) {
+    v += __shfl_down_sync(0xffffffffu, v, o);
+    f += __shfl_down_sync(0xffffffffu, f, o);
+    sum += __shfl_down_sync(0xffffffffu, sum, o);
+    const unsigned long long m2 = __shfl_down_sync(0xffffffffu, mx, o);
+    if (m2 > mx) mx = m2;
+  }
+  if (lane == 0) {
+    agg[4 * r] = v;
+    agg[4 * r + 1] = f;
+    agg[4 * r + 2] = mx;
+    agg[4 * r + 3] = sum;
+  }
+}
+
+cudaError_t launch_segment_reduce(const uint64_t* p, const uint64_t* off, uint32_t nreq,
+                                  unsigned long long* agg, cudaStream_t s) {
+  if (!nreq) return cudaSuccess;
+  segment_reduce_kernel<<<(nreq + 7) / 8, 256, 0, s>>>(p, off, nreq, agg);
+  return cudaGetLastError();
+}
+
 __global__ void is_prime_kernel(const uint64_t* n, uint64_t count, uint8_t* out) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
        i += (uint64_t)gridDim.x * blockDim.x)

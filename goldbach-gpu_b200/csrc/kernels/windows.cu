@@ -45,6 +45,32 @@ __device__ __forceinline__ uint32_t find_window(const uint64_t* off, uint32_t nw
   return lo;
 }
 
+// Per-window sieving bound: nsieve = #primes <= isqrt(q_top) (binary search
+// in the resident table), so the host never looks these up one by one.
+__global__ void win_nsieve_kernel(WinDesc* win, uint32_t nwin, const uint32_t* primes,
+                                  uint64_t nprimes) {
+  const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= nwin) return;
+  const uint64_t q = win[w].q_top;
+  uint64_t r = (uint64_t)sqrt((double)q);
+  while (r > 0 && (r > 0xffffffffull || r * r > q)) --r;
+  while (r < 0xffffffffull && (r + 1) * (r + 1) <= q) ++r;
+  uint64_t lo = 0, hi = nprimes;  // first index with primes[i] > r
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if (primes[mid] <= r) lo = mid + 1;
+    else hi = mid;
+  }
+  win[w].nsieve = (uint32_t)(lo > kWheelPrimeCount + 1 ? lo : kWheelPrimeCount + 1);
+}
+
+cudaError_t launch_win_nsieve(WinDesc* win, uint32_t nwin, const uint32_t* primes, uint64_t nprimes,
+                              cudaStream_t s) {
+  if (!nwin) return cudaSuccess;
+  win_nsieve_kernel<<<(nwin + 255) / 256, 256, 0, s>>>(win, nwin, primes, nprimes);
+  return cudaGetLastError();
+}
+
 // A. tile sieve ---------------------------------------------------------------
 __global__ void __launch_bounds__(kWinThreads) win_tile_kernel(const __grid_constant__ WindowsArgs a,
                                                                uint32_t w_only) {

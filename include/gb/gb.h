@@ -254,6 +254,80 @@ gb_status gb_verify_windows(gb_ctx* ctx, const gb_window* w, size_t count,
                             const gb_windows_opts* opts, gb_window_result* res,
                             uint32_t* min_p_concat, gb_windows_summary* sum);
 
+/* -------------------------------------------------------------------------
+ * Serving: a request loop with continuous batching.
+ *
+ * The reference serves one query per process (`single_check <n>`, or a
+ * `goldbach --start=A L` run).  Here requests are submitted from any thread
+ * and complete independently.  Two lanes run concurrently on their own
+ * streams over the context's resident tables: the single lane runs single
+ * n and short ranges (n by n) through the single-n kernel; the range lane
+ * runs the other ranges through the windows pipeline.  A lane takes every
+ * request that is waiting when its previous batch finishes, in arrival
+ * order, as far as its batch size and its device memory (an arena reserved
+ * at start) allow; requests that arrive meanwhile join the lane's next
+ * batch.  Each result depends only on its own request.
+ * ---------------------------------------------------------------------- */
+#define GB_REQ_SINGLE 0 /* n = a (even, >= 4)                       */
+#define GB_REQ_RANGE 1  /* every even n in [a, a + 2*(count-1)]      */
+
+typedef struct gb_request {
+  int kind;
+  uint64_t a;
+  uint64_t count;      /* GB_REQ_RANGE: even n in the range (>= 1)       */
+  uint64_t arrival_ns; /* on gb_now_ns()'s clock; 0: at submission        */
+} gb_request;
+
+typedef struct gb_response {
+  gb_status status;
+  int kind;
+  uint64_t p, q;      /* single: minimal partition (p = 0: none <= bound) */
+  uint64_t verified;  /* range: n with a partition (single: 0 or 1)       */
+  uint64_t failures;
+  uint64_t max_minp;
+  uint64_t minp_sum;  /* sum of minimal p over the request                */
+  double latency_us;  /* arrival to completion                            */
+  uint32_t lane;      /* 0: single lane, 1: range lane                    */
+  uint32_t batch;     /* the lane batch that served it                    */
+} gb_response;
+
+typedef struct gb_serve_opts {
+  uint64_t max_n;              /* largest n served (0: 2^64 - 1)               */
+  uint32_t max_single_batch;   /* n per single-lane batch (0: 2^18)            */
+  uint32_t max_range_batch;    /* requests per range-lane batch (0: 4096)      */
+  uint64_t range_arena_bytes;  /* range-lane device memory (0: 4 GiB)          */
+  uint64_t small_range;        /* ranges of <= this many n run n by n (0: 2^15) */
+} gb_serve_opts;
+
+typedef struct gb_serve_stats {
+  uint64_t submitted, completed, pending, rejected;
+  uint64_t batches_single, batches_range;
+  double p50_us, p99_us, max_us, mean_us; /* latency of completed requests */
+  double elapsed_s;                       /* since start or last reset       */
+  double completed_per_s;
+} gb_serve_stats;
+
+/* Measured peaks for the roofline of the integer kernels: 32-bit ALU
+ * operations per second and conflict-free shared-memory atomicAnd per second
+ * on this device (short probe kernels; no counterpart in the reference). */
+gb_status gb_probe_peaks(gb_ctx* ctx, double* alu_ops_per_s, double* smem_atomics_per_s);
+
+/* Monotonic clock used for arrival times (nanoseconds). */
+uint64_t gb_now_ns(void);
+/* Starts the serving lanes on ctx (builds the tables for max_n first). */
+gb_status gb_serve_start(gb_ctx* ctx, const gb_serve_opts* opts);
+/* Queues count requests; tickets[i] identifies request i.  Thread-safe. */
+gb_status gb_submit(gb_ctx* ctx, const gb_request* reqs, size_t count, uint64_t* tickets);
+/* GB_OK and the response once done (the ticket is then released),
+ * GB_EAGAIN while pending.  Thread-safe. */
+gb_status gb_poll(gb_ctx* ctx, uint64_t ticket, gb_response* out);
+/* Like gb_poll, waiting up to timeout_ms (GB_ETIMEOUT after that). */
+gb_status gb_wait(gb_ctx* ctx, uint64_t ticket, gb_response* out, uint64_t timeout_ms);
+/* Latency percentiles and throughput; reset != 0 starts a new window. */
+gb_status gb_serve_stats_get(gb_ctx* ctx, gb_serve_stats* out, int reset);
+/* Drains the pending requests and stops the lanes. */
+gb_status gb_serve_stop(gb_ctx* ctx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,65 @@
+"""Serving with continuous batching: every response equals the same request
+run alone (single n: gb_check_single_batch; range: gb_verify_range), while
+requests of both kinds are queued, batched and overlapped on the GPU."""
+import time
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _alone(ctx, kind, a, count):
+    if kind == 0:
+        p, q, _ = ctx.check_single(np.array([a], np.uint64))
+        return {"p": int(p[0]), "q": int(q[0]), "verified": int(p[0] > 0),
+                "failures": int(p[0] == 0), "max_minp": int(p[0]), "minp_sum": int(p[0])}
+    r = ctx.verify_range(a, a + 2 * (count - 1), want_minp=True)
+    m = r.min_p.astype(np.uint64)
+    return {"verified": int((m > 0).sum()), "failures": int((m == 0).sum()),
+            "max_minp": int(m.max()), "minp_sum": int(m.sum())}
+
+
+def test_mixed_stream_matches_requests_run_alone(gbmod):
+    with gbmod.Context(0, max_n=10**13) as ctx:
+        ctx.serve_start(max_n=10**13, small_range=2000, max_single_batch=1 << 16)
+        rng = np.random.default_rng(3)
+        reqs = []
+        for _ in range(3):  # three waves: later ones arrive while earlier run
+            for _ in range(200):
+                reqs.append((0, int(rng.integers(2, 5 * 10**12)) * 2, 1))
+            for _ in range(30):
+                reqs.append((1, int(rng.integers(2, 5 * 10**12)) * 2, int(rng.integers(1, 2000))))
+            for _ in range(8):
+                reqs.append((1, int(rng.integers(2, 5 * 10**12)) * 2, int(rng.integers(2001, 300000))))
+        tickets = []
+        for w in range(3):
+            part = reqs[w * 238:(w + 1) * 238]
+            k, a, c = zip(*part)
+            tickets += list(ctx.submit(k, a, c))
+            time.sleep(0.002)
+        got = [ctx.wait(t, 120000) for t in tickets]
+        st = ctx.serve_stats()
+        assert st["completed"] == st["submitted"] == len(reqs)
+        assert st["rejected"] == 0 and st["p99_us"] >= st["p50_us"] > 0
+        lanes = {g["lane"] for g in got}
+        assert lanes == {0, 1}
+        for (kind, a, count), g in zip(reqs, got):
+            assert g["status"] == 0
+            want = _alone(ctx, kind, a, count)
+            for key, v in want.items():
+                assert g[key] == v, (kind, a, count, key, g[key], v)
+        ctx.serve_stop()
+
+
+def test_invalid_requests_are_rejected_not_run(gbmod):
+    with gbmod.Context(0, max_n=10**12) as ctx:
+        ctx.serve_start(max_n=10**12)
+        t = ctx.submit([0, 0, 1, 0], [7, 2, 10, 2 * 10**12], [1, 1, 0, 1])
+        res = [ctx.wait(x, 10000) for x in t]
+        assert [r["status"] for r in res] == [gbmod.GB_EINVAL] * 4
+        ok = ctx.submit([0], [100])[0]
+        r = ctx.wait(ok, 10000)
+        assert r["status"] == 0 and r["p"] + r["q"] == 100 and r["p"] == 3
+        assert ctx.serve_stats()["rejected"] == 4
+        ctx.serve_stop()
