@@ -44,7 +44,7 @@ struct WheelGroup {
 // Pattern storage: each group stores bits [0, period + 64) of its periodic
 // pattern (bit b = 1 iff 2g+1 has no factor in the group for g = b mod period),
 // rounded up to whole words plus one spare word for the funnel shift.
-constexpr uint32_t wheel_words(uint32_t period) { return (period + 64 + 31) / 32 + 1; }
+GB_HD constexpr uint32_t wheel_words(uint32_t period) { return (period + 64 + 31) / 32 + 1; }
 
 constexpr uint32_t kP0 = 3 * 5 * 7 * 11 * 13;  // 15015
 constexpr uint32_t kP1 = 17 * 19 * 23;         // 7429
@@ -74,6 +74,27 @@ GB_HD constexpr uint32_t wheel_period(int x) {
 }
 GB_HD constexpr uint32_t wheel_offset(int x) {
   return x == 0 ? kO0 : x == 1 ? kO1 : x == 2 ? kO2 : x == 3 ? kO3 : x == 4 ? kO4 : x == 5 ? kO5 : kO6;
+}
+
+// ---------------------------------------------------------------------------
+// Mod-6 layout.  Odd q not divisible by 3 are 6G+1 or 6G+5; the two class
+// bitsets hold bit t <-> q = 6(G0+t)+c, c in {1, 5}.  The wheel for the
+// primes 5..67 becomes one periodic pattern per (class, group) indexed by
+// G mod period: bit x = 1 iff 6x+c has no factor in the group.
+constexpr int kWheel6Groups = 7;
+constexpr uint32_t kQ0 = 5 * 7 * 11 * 13;  // 5005
+GB_HD constexpr uint32_t wheel6_period(int x) {
+  return x == 0 ? kQ0 : x == 1 ? kP1 : x == 2 ? kP2 : x == 3 ? kP3 : x == 4 ? kP4 : x == 5 ? kP5 : kP6;
+}
+GB_HD constexpr uint32_t wheel6_group_offset(int x) {
+  uint32_t o = 0;
+  for (int i = 0; i < x; ++i) o += wheel_words(wheel6_period(i));
+  return o;
+}
+constexpr uint32_t kWheel6ClassWords = wheel6_group_offset(kWheel6Groups);
+constexpr uint32_t kWheel6Words = 2 * kWheel6ClassWords;  // class 1 groups, then class 5
+GB_HD constexpr uint32_t wheel6_offset(int cls5, int x) {
+  return (cls5 ? kWheel6ClassWords : 0) + wheel6_group_offset(x);
 }
 
 // ---------------------------------------------------------------------------

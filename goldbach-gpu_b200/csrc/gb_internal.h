@@ -64,6 +64,11 @@ struct RangeArgs {
   uint32_t nsieve;         // primes[kWheelPrimeCount+1 .. nsieve) mark the window
   uint32_t kcoop;          // ... those below kcoop warp-cooperatively
   const uint32_t* wheel;   // wheel pattern table (kWheelWords)
+  // mod-6 layout (range6_kernel): class wheel patterns, per-prime class
+  // offsets, and the bits each class bitset marks
+  int layout6;
+  const uint32_t* wheel6;  // kWheel6Words
+  const uint2* a15;
 };
 
 struct SieveArgs {
@@ -110,12 +115,12 @@ struct WindowsArgs {
 };
 
 // kernels/tables.cu
-cudaError_t launch_wheel_init(uint32_t* wheel, cudaStream_t s);
+cudaError_t launch_wheel_init(uint32_t* wheel, uint32_t* wheel6, cudaStream_t s);
 cudaError_t launch_sieve_bits(const SieveArgs& a, cudaStream_t s);
 // Appends the primes of `bits` (odd-only from q_lo) after `prefix` entries of
 // `primes`; writes the new total into *d_total (device) and magic[] for them.
 cudaError_t launch_compact_primes(const uint32_t* bits, uint64_t nbits, uint64_t q_lo,
-                                  uint32_t* primes, uint64_t* magic, uint64_t prefix,
+                                  uint32_t* primes, uint64_t* magic, uint2* a15, uint64_t prefix,
                                   uint64_t cap, unsigned long long* d_total,
                                   uint32_t* scratch_blocks, uint32_t nblocks_cap,
                                   cudaStream_t s);

@@ -171,22 +171,26 @@ gb_status ensure_primes(gb_ctx* c, Workspace& w, uint64_t limit) {
   const size_t nblk = compact_scratch_blocks(nbits_max);
   uint32_t* primes = nullptr;
   uint64_t* magic = nullptr;
+  uint2* a15 = nullptr;
   Temps t(c, nullptr);
   uint32_t *bits, *blocks;
   unsigned long long* total;
   gb_status st;
   if ((st = dev_alloc(c, (void**)&primes, cap * 4, &w.err)) != GB_OK) return st;
   if ((st = dev_alloc(c, (void**)&magic, cap * 8, &w.err)) != GB_OK ||
+      (st = dev_alloc(c, (void**)&a15, cap * 8, &w.err)) != GB_OK ||
       (st = t.get(((nbits_max + 31) / 32 + 4) * 4, (void**)&bits, w)) != GB_OK ||
       (st = t.get((nblk + 1) * 4, (void**)&blocks, w)) != GB_OK ||
       (st = t.get(8, (void**)&total, w)) != GB_OK) {
     dev_free(c, primes);
     dev_free(c, magic);
+    dev_free(c, a15);
     return st;
   }
   auto bail = [&](cudaError_t e, const char* what) {
     dev_free(c, primes);
     dev_free(c, magic);
+    dev_free(c, a15);
     return cuda_fail(w, e, what);
   };
   uint64_t cur = 0, count = 0;
@@ -215,7 +219,7 @@ gb_status ensure_primes(gb_ctx* c, Workspace& w, uint64_t limit) {
     a.out = bits;
     cudaError_t e = launch_sieve_bits(a, c->stream);
     if (e == cudaSuccess)
-      e = launch_compact_primes(bits, nbits, 3, primes, magic, 1, cap, total, blocks,
+      e = launch_compact_primes(bits, nbits, 3, primes, magic, a15, 1, cap, total, blocks,
                                 (uint32_t)(nblk + 1), c->stream);
     unsigned long long tot = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&tot, total, 8, cudaMemcpyDeviceToHost, c->stream);
@@ -232,8 +236,10 @@ gb_status ensure_primes(gb_ctx* c, Workspace& w, uint64_t limit) {
   t.release();
   dev_free(c, c->d_primes);
   dev_free(c, c->d_magic);
+  dev_free(c, c->d_a15);
   c->d_primes = primes;
   c->d_magic = magic;
+  c->d_a15 = a15;
   c->nprimes = count;
   c->primes_limit = target;
   const uint64_t nh = std::min<uint64_t>(count, pi_upper(kHostPrimeLimit));
@@ -270,7 +276,9 @@ gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint
     return fail(w, GB_EINVAL, "halo must be a multiple of 64 in [128, 2^17]");
   uint32_t NE = o.chunk_evens;
   if (!NE) {
-    NE = 1u << 19;
+    // the mod-6 window is 2/3 the size of the odd-only one: 2^20 n fit two
+    // CTAs per SM
+    NE = kRangeLayout6 ? 1u << 20 : 1u << 19;
     while (NE > 8192 && NE / 2 >= count) NE >>= 1;
   }
   if (NE < 8192 || NE > (1u << 20) || (NE & (NE - 1)))
@@ -295,12 +303,24 @@ gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint
   a.chunks_per_seg = cps;
   a.total_items = my_segs * cps;
   a.chunk_evens = NE;
-  a.nbw = (H / 2 + NE) / 32 + 2;
+  a.layout6 = kRangeLayout6;
+  uint64_t search_top, window_bits;
+  if (kRangeLayout6) {
+    // two class bitsets of H/6 + NE/3 bits (plus the funnel over-read of the
+    // last warp task); primes p <= H - 13 keep every q = n - p in the window
+    a.nbw = (H / 6 + 96) / 32 + 1 + (((NE / 3 + 2) / 32 + 256) & ~255u) + 4;
+    search_top = std::min<uint64_t>(H - 13, p_lim);
+    window_bits = H / 6 + NE / 3;
+  } else {
+    a.nbw = (H / 2 + NE) / 32 + 2;
+    search_top = std::min<uint64_t>(H - 1, p_lim);
+    window_bits = H / 2 + NE;
+  }
   uint64_t ns = 0, kf = 0, nsv = 0, kc = 0;
-  if ((st = count_le(c, w, std::min<uint64_t>(H - 1, p_lim), &ns)) != GB_OK ||
+  if ((st = count_le(c, w, search_top, &ns)) != GB_OK ||
       (st = count_le(c, w, o.p_small, &kf)) != GB_OK ||
       (st = count_le(c, w, root, &nsv)) != GB_OK ||
-      (st = count_le(c, w, (H / 2 + NE) / 64, &kc)) != GB_OK)
+      (st = count_le(c, w, window_bits / 64, &kc)) != GB_OK)
     return st;
   sp.halo = H;
   sp.nsearch = (uint32_t)ns;
@@ -318,6 +338,8 @@ gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint
   a.nsieve = (uint32_t)std::max<uint64_t>(nsv, kWheelPrimeCount + 1);
   a.kcoop = (uint32_t)std::max<uint64_t>(kc, kWheelPrimeCount + 1);
   a.wheel = c->d_wheel;
+  a.wheel6 = c->d_wheel6;
+  a.a15 = c->d_a15;
 
   cudaStream_t s = o.stream ? (cudaStream_t)o.stream : c->stream;
   gb_range_out od{};
@@ -547,7 +569,7 @@ uint64_t gb_estimate_device_bytes(const gb_config* cfg) {
   const uint64_t np = pi_upper(want);
   // primes + reciprocals, the build bitset and scan blocks, wheel, counters,
   // histogram and the Phase-2 queue
-  return np * 12 + want / 16 + (want / 65536 + 1) * 4 + kWheelWords * 4 + kCtrCount * 8 +
+  return np * 20 + want / 16 + (want / 65536 + 1) * 4 + kWheelWords * 4 + kCtrCount * 8 +
          GB_HIST_BINS * 8 + (1ull << 20) * sizeof(QEntry);
 }
 
@@ -573,8 +595,10 @@ gb_status gb_create(int device, const gb_config* cfg, gb_ctx** out) {
   size_t fr = 0, tot = 0;
   cudaMemGetInfo(&fr, &tot);
   c->budget = (cfg && cfg->device_mem_budget) ? cfg->device_mem_budget : (uint64_t)fr;
-  if (dev_alloc(c, (void**)&c->d_wheel, kWheelWords * 4) != GB_OK) return bail(GB_ENOMEM);
-  if (launch_wheel_init(c->d_wheel, c->stream) != cudaSuccess) return bail(GB_ECUDA);
+  if (dev_alloc(c, (void**)&c->d_wheel, kWheelWords * 4) != GB_OK ||
+      dev_alloc(c, (void**)&c->d_wheel6, kWheel6Words * 4) != GB_OK)
+    return bail(GB_ENOMEM);
+  if (launch_wheel_init(c->d_wheel, c->d_wheel6, c->stream) != cudaSuccess) return bail(GB_ECUDA);
   gb_status st = ws_init(c, c->ws, 1u << 20);
   if (st != GB_OK) return bail(st);
   uint64_t want = GB_PHASE2_LIMIT_DEFAULT;

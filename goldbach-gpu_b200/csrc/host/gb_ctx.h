@@ -62,9 +62,11 @@ struct gb_ctx {
   std::string err;
 
   // resident tables (read-only while any lane runs)
-  uint32_t* d_wheel = nullptr;
+  uint32_t* d_wheel = nullptr;   // odd-only wheel patterns
+  uint32_t* d_wheel6 = nullptr;  // mod-6 class wheel patterns
   uint32_t* d_primes = nullptr;  // all primes <= primes_limit, ascending, 2 first
   uint64_t* d_magic = nullptr;   // Barrett reciprocals, one per prime
+  uint2* d_a15 = nullptr;        // mod-6 class offsets (-1/6, -5/6 mod p), one per prime
   uint64_t nprimes = 0;
   uint64_t primes_limit = 0;
   std::vector<uint32_t> h_primes;  // host copy of the primes <= kHostPrimeLimit
@@ -80,6 +82,9 @@ constexpr uint64_t kHostPrimeLimit = 1ull << 22;
 constexpr uint64_t kSampleStride = 1024;
 // primes searched word-parallel (lockstep) before the per-n tail
 constexpr uint64_t kLockPrimes = 128;
+// range kernel window layout: true = mod-6 class bitsets (range6_kernel),
+// false = odd-only bitset (range_kernel)
+constexpr bool kRangeLayout6 = true;
 
 gb_status fail(Workspace& w, gb_status st, const std::string& msg);
 gb_status cuda_fail(Workspace& w, cudaError_t e, const char* what);

@@ -21,6 +21,8 @@
 #include "../gb_internal.h"
 #include "gb/gb.h"
 #include "search.cuh"
+#include "search6.cuh"
+#include "sieve6.cuh"
 #include "sieve_window.cuh"
 
 namespace gb {
@@ -77,6 +79,91 @@ __global__ void __launch_bounds__(kRangeThreads, 2) range_kernel(const __grid_co
     sieve_window<kRangeThreads>(Q, a.nbw, nbits, g0, q_top, pat, s.primes, a.magic, a.nsieve,
                                 a.kcoop);
     search_chunk<MINP, kRangeThreads>(s, Q, SOFF, HIST, c, &s_fb, &s_maxp, &s_psum);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The same fused kernel on the mod-6 layout (sieve6.cuh, search6.cuh): the
+// q-window is the two class bitsets Q1 / Q5 (no multiple of 3 stored), and
+// the n of a chunk are searched by class n mod 6.
+
+// floor((A - H - 1) / 6) for A possibly below H
+__device__ __forceinline__ int64_t window_g0(uint64_t A, uint32_t H) {
+  if (A >= (uint64_t)H + 1) return (int64_t)((A - H - 1) / 6);
+  return -(int64_t)(((uint64_t)H + 1 - A + 5) / 6);
+}
+
+template <bool MINP>
+__global__ void __launch_bounds__(kRangeThreads, 2) range6_kernel(const __grid_constant__ RangeArgs a) {
+  extern __shared__ uint32_t smem[];
+  const SearchParams& s = a.s;
+  uint32_t* pat6 = smem;
+  uint32_t* Q1 = pat6 + kWheel6Words;
+  uint32_t* Q5 = Q1 + a.nbw;
+  uint32_t* HIST = Q5 + a.nbw;
+  uint32_t* E0 = HIST + kSmemHistBins;
+  uint32_t* E2 = E0 + kLockSteps6;
+  uint32_t* E4 = E2 + kLockSteps6;
+  __shared__ Ctx6 cx;
+  __shared__ unsigned long long s_item;
+  const int tid = threadIdx.x;
+
+  for (uint32_t i = tid; i < kWheel6Words; i += kRangeThreads) pat6[i] = a.wheel6[i];
+  if (tid == 0) {
+    cx.Q1 = Q1;
+    cx.Q5 = Q5;
+    cx.HIST = HIST;
+  }
+  load_tables6(s, &cx, E0, E2, E4);
+  const Smem6 sm{Q1, Q5, HIST, E0, E2, E4};
+
+  for (;;) {
+    if (tid == 0) {
+      s_item = atomicAdd(&s.ctr[kCtrWork], 1ull);
+      cx.fb = 0;
+      cx.maxp = 0;
+      cx.psum = 0;
+      cx.next_task = 0;
+    }
+    for (uint32_t i = tid; i < kSmemHistBins; i += kRangeThreads) HIST[i] = 0;
+    __syncthreads();
+    const unsigned long long item = s_item;
+    if (item >= a.total_items) break;
+    const uint64_t ls = item / a.chunks_per_seg;
+    const uint64_t ci = item - ls * a.chunks_per_seg;
+    const uint64_t seg = a.shard_index + ls * a.shard_count;
+    const uint64_t seg_first = seg * a.seg_size;
+    const uint64_t seg_rem = a.total_count - seg_first;
+    const uint64_t seg_cnt = seg_rem < a.seg_size ? seg_rem : a.seg_size;
+    const uint64_t j0 = ci * a.chunk_evens;
+    if (j0 >= seg_cnt) {
+      __syncthreads();
+      continue;
+    }
+    const uint64_t A = a.start + 2 * (seg_first + j0);
+    const uint32_t cnt = (uint32_t)(seg_cnt - j0 < a.chunk_evens ? seg_cnt - j0 : a.chunk_evens);
+    const int64_t G0 = window_g0(A, s.halo);
+    if (tid == 0) {
+      cx.A = A;
+      cx.base_idx = seg_first + j0;
+      cx.unit = seg;
+      const uint64_t last = A + 2ull * (cnt - 1);
+      const uint32_t amod = (uint32_t)(A % 6);
+      // A - 6 G0 is in [H + 1, H + 7), so every X fits 32 bits
+      const uint32_t a6 = (uint32_t)((int64_t)A - 6 * G0);
+#pragma unroll
+      for (int ri = 0; ri < 3; ++ri) {
+        const uint32_t d = (uint32_t)((2 * ri - (int)amod + 6) % 6);
+        cx.n[ri] = A + d;
+        cx.M[ri] = last >= A + d ? (uint32_t)((last - A - d) / 6 + 1) : 0u;
+        cx.X[ri][0] = a6 + d - 1;
+        cx.X[ri][1] = a6 + d - 5;
+      }
+    }
+    const uint32_t nbits = s.halo / 6 + cnt / 3 + 96;
+    sieve_window6<kRangeThreads>(Q1, Q5, a.nbw, nbits, G0, A + 2ull * cnt, pat6, s.primes,
+                                 a.magic, a.a15, a.nsieve, a.kcoop);
+    search_chunk6<MINP, kRangeThreads>(s, sm, &cx);
   }
 }
 
@@ -141,37 +228,41 @@ __global__ void __launch_bounds__(kFallbackThreads) fallback_kernel(const __grid
 
 // ---------------------------------------------------------------------------
 size_t range_smem_bytes(const RangeArgs& a) {
+  if (a.layout6)
+    return (size_t)(kWheel6Words + 2 * a.nbw + kSmemHistBins + 3 * kLockSteps6) * sizeof(uint32_t);
   return (size_t)(kWheelWords + a.nbw + kSmemHistBins) * sizeof(uint32_t) +
          (size_t)((a.s.nsearch + 1) & ~1u) * sizeof(uint16_t);
 }
 
-template <bool MINP>
-static int occupancy(size_t smem) {
+template <typename K>
+static int occupancy(K kernel, size_t smem) {
   int nb = 0;
-  cudaFuncSetAttribute(range_kernel<MINP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, range_kernel<MINP>, kRangeThreads, smem);
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, kRangeThreads, smem);
   return nb;
 }
 
 int range_max_blocks_per_sm(const RangeArgs& a) {
   const size_t smem = range_smem_bytes(a);
-  return a.s.minp ? occupancy<true>(smem) : occupancy<false>(smem);
+  if (a.layout6) return a.s.minp ? occupancy(range6_kernel<true>, smem) : occupancy(range6_kernel<false>, smem);
+  return a.s.minp ? occupancy(range_kernel<true>, smem) : occupancy(range_kernel<false>, smem);
+}
+
+template <typename K>
+static cudaError_t launch_one(K kernel, const RangeArgs& a, int grid, size_t smem, cudaStream_t st) {
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kernel<<<grid, kRangeThreads, smem, st>>>(a);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_range(const RangeArgs& a, int grid, cudaStream_t st) {
   const size_t smem = range_smem_bytes(a);
-  if (a.s.minp) {
-    cudaError_t e = cudaFuncSetAttribute(range_kernel<true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    range_kernel<true><<<grid, kRangeThreads, smem, st>>>(a);
-  } else {
-    cudaError_t e = cudaFuncSetAttribute(range_kernel<false>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    range_kernel<false><<<grid, kRangeThreads, smem, st>>>(a);
-  }
-  return cudaGetLastError();
+  if (a.layout6)
+    return a.s.minp ? launch_one(range6_kernel<true>, a, grid, smem, st)
+                    : launch_one(range6_kernel<false>, a, grid, smem, st);
+  return a.s.minp ? launch_one(range_kernel<true>, a, grid, smem, st)
+                  : launch_one(range_kernel<false>, a, grid, smem, st);
 }
 
 cudaError_t launch_fallback(const SearchParams& s, int grid, cudaStream_t st) {

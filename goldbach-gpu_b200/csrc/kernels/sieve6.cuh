@@ -1,0 +1,164 @@
+// sieve6.cuh -- mod-6 window sieve in shared memory (sm_100a).
+//
+// Same job as sieve_window.cuh (and as the reference's
+// tiled_sieve_segment_kernel, src/goldbach.cu:198-259), on a layout that
+// never stores a multiple of 3: the window's odd q not divisible by 3 are
+// split into two class bitsets,
+//     Q1: bit t <-> q = 6(G0+t) + 1,      Q5: bit t <-> q = 6(G0+t) + 5,
+// which together hold 1/3 of the numbers (the odd-only layout holds 1/2).
+// Each prime p >= 5 has one multiple in every 6p numbers per class, so in
+// both bitsets its multiples are p bits apart: the sieve marks 2/3 of the
+// bits it would mark odd-only.  The first multiple in a window costs one
+// Barrett reduction r = G0 mod p for both classes, using the per-prime class
+// offsets a1 = -1/6 and a5 = -5/6 (mod p) kept with the prime table:
+//     6(G0+t) + c == 0 (mod p)  <=>  t == a_c - r (mod p).
+#pragma once
+#include "../gb_device.cuh"
+
+namespace gb {
+
+// First t >= 0 of class c (offset a_c, r = G0 mod p) whose q is >= p^2.
+__device__ __forceinline__ uint64_t first_mark6(int64_t G0, uint32_t p, uint32_t ac, uint32_t r,
+                                               uint32_t c) {
+  uint64_t t = ac >= r ? ac - r : ac + p - r;
+  // q(t) = 6(G0 + t) + c is below p^2 only in windows that start below p^2;
+  // compared in G (q itself may not fit an int64 near 2^64)
+  const uint64_t pp = (uint64_t)p * p;
+  const int64_t gmin = (int64_t)((pp - c + 5) / 6);  // first G with 6G + c >= p^2
+  if (G0 + (int64_t)t < gmin) {
+    const int64_t tmin = gmin - G0;
+    t += (uint64_t)p * (((uint64_t)(tmin - (int64_t)t) + p - 1) / p);
+  }
+  return t;
+}
+
+// First marks of p in both classes as 32-bit offsets, lim (>= every
+// in-window offset) when there is none below it.  The p^2 clamp of
+// first_mark6 is needed only when the window starts below p^2 + 4 (6 G0 is
+// compared, not computed per class).
+__device__ __forceinline__ void first_marks6(int64_t G0, uint32_t p, uint2 ac, uint32_t r,
+                                             uint32_t lim, uint32_t& t1, uint32_t& t5) {
+  const uint64_t pp = (uint64_t)p * p;
+  if (G0 < 0 || 6 * (uint64_t)G0 < pp + 4) {
+    const uint64_t f1 = first_mark6(G0, p, ac.x, r, 1);
+    const uint64_t f5 = first_mark6(G0, p, ac.y, r, 5);
+    t1 = f1 < lim ? (uint32_t)f1 : lim;
+    t5 = f5 < lim ? (uint32_t)f5 : lim;
+  } else {
+    const uint32_t a = ac.x >= r ? ac.x - r : ac.x + p - r;  // < p
+    const uint32_t b = ac.y >= r ? ac.y - r : ac.y + p - r;
+    t1 = a < lim ? a : lim;
+    t5 = b < lim ? b : lim;
+  }
+}
+
+// r = G0 mod p for a signed window base.
+__device__ __forceinline__ uint32_t base_mod(int64_t G0, uint32_t p, uint64_t magic) {
+  if (G0 >= 0) return mod_p((uint64_t)G0, p, magic);
+  const uint32_t m = mod_p((uint64_t)(-G0), p, magic);
+  return m ? p - m : 0;
+}
+
+// Sieves bits [0, nbits) of both class bitsets (nwords words each written).
+// Exact for every q <= q_top.  pat6: the class wheel patterns (shared
+// memory).  primes[kWheelPrimeCount+1 .. nsieve) are the marking primes
+// (71, 73, ...), those below kcoop marked warp-cooperatively.  Ends with
+// __syncthreads().
+template <int NT>
+__device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ Q5,
+                              uint32_t nwords, uint32_t nbits, int64_t G0, uint64_t q_top,
+                              const uint32_t* __restrict__ pat6,
+                              const uint32_t* __restrict__ primes,
+                              const uint64_t* __restrict__ magic, const uint2* __restrict__ a15,
+                              uint32_t nsieve, uint32_t kcoop) {
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  constexpr int NW = NT / 32;
+
+  // 1. wheel fill of both classes: word t covers G0 + 32t .. +31.
+#pragma unroll
+  for (int cls5 = 0; cls5 < 2; ++cls5) {
+    uint32_t* Q = cls5 ? Q5 : Q1;
+    uint32_t r[kWheel6Groups];
+    const int64_t g = G0 + 32 * (int64_t)tid;
+#pragma unroll
+    for (int x = 0; x < kWheel6Groups; ++x) {
+      const int64_t P = wheel6_period(x);
+      int64_t m = g % P;
+      if (m < 0) m += P;
+      r[x] = (uint32_t)m;
+    }
+    for (uint32_t t = tid; t < nwords; t += NT) {
+      uint32_t w = 0xffffffffu;
+#pragma unroll
+      for (int x = 0; x < kWheel6Groups; ++x) {
+        const uint32_t P = wheel6_period(x);
+        const uint32_t step = (uint32_t)((32ull * NT) % P);
+        const uint32_t rr = r[x];
+        const uint32_t* pp = pat6 + wheel6_offset(cls5, x) + (rr >> 5);
+        w &= __funnelshift_r(pp[0], pp[1], rr & 31);
+        const uint32_t nr = rr + step;
+        r[x] = nr >= P ? nr - P : nr;
+      }
+      Q[t] = w;
+    }
+  }
+  __syncthreads();
+
+  // 2. the first window: q < 5 (1 and below) is not prime, and the primes
+  //    5..67 were cleared by their own patterns (q = 6G + c < 72 <=> G < 12).
+  if (G0 < 12) {
+    const int64_t hi = 12 - G0 < (int64_t)nbits ? 12 - G0 : (int64_t)nbits;
+    for (int64_t i = tid; i < 2 * hi; i += NT) {
+      const int cls5 = (int)(i >= hi);
+      const int64_t t = cls5 ? i - hi : i;
+      const int64_t q = 6 * (G0 + t) + (cls5 ? 5 : 1);
+      bool prime = q >= 5;
+      for (int d = 5; prime && d * d <= q; d += 2)
+        if (q % d == 0) prime = false;
+      uint32_t* Q = cls5 ? Q5 : Q1;
+      const uint32_t bit = 1u << (t & 31);
+      if (prime) atomicOr(&Q[t >> 5], bit);
+      else atomicAnd(&Q[t >> 5], ~bit);
+    }
+    __syncthreads();
+  }
+
+  // 3. primes with many multiples: one warp per prime, both classes
+  //    (stride 32p stays far below 2^32: these primes are < nbits / 64).
+  const uint32_t kfirst = kWheelPrimeCount + 1;
+  const uint32_t kc = kcoop < nsieve ? kcoop : nsieve;
+  for (uint32_t k = kfirst + warp; k < kc; k += NW) {
+    const uint32_t p = __ldg(primes + k);
+    if ((uint64_t)p * p > q_top) break;
+    uint32_t t1, t5;
+    first_marks6(G0, p, __ldg(a15 + k), base_mod(G0, p, __ldg(magic + k)), nbits, t1, t5);
+    const uint32_t stride = 32 * p;
+    for (uint32_t i = t1 + lane * p; i < nbits; i += stride)
+      atomicAnd(&Q1[i >> 5], ~(1u << (i & 31)));
+    for (uint32_t i = t5 + lane * p; i < nbits; i += stride)
+      atomicAnd(&Q5[i >> 5], ~(1u << (i & 31)));
+  }
+  // 4. one thread per prime for the rest, both classes in one loop; the
+  //    steps are taken only while they stay below nbits (p may be near 2^32).
+  for (uint32_t k = (kc > kfirst ? kc : kfirst) + tid; k < nsieve; k += NT) {
+    const uint32_t p = __ldg(primes + k);
+    if ((uint64_t)p * p > q_top) break;
+    uint32_t j1, j5;
+    first_marks6(G0, p, __ldg(a15 + k), base_mod(G0, p, __ldg(magic + k)), nbits, j1, j5);
+    while (j1 < nbits || j5 < nbits) {
+      if (j1 < nbits) {
+        atomicAnd(&Q1[j1 >> 5], ~(1u << (j1 & 31)));
+        j1 = nbits - j1 > p ? j1 + p : nbits;
+      }
+      if (j5 < nbits) {
+        atomicAnd(&Q5[j5 >> 5], ~(1u << (j5 & 31)));
+        j5 = nbits - j5 > p ? j5 + p : nbits;
+      }
+    }
+  }
+  __syncthreads();
+}
+
+}  // namespace gb

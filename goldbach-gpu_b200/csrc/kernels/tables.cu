@@ -52,8 +52,38 @@ __global__ void wheel_init_kernel(uint32_t* wheel) {
   wheel[W] = v;
 }
 
-cudaError_t launch_wheel_init(uint32_t* wheel, cudaStream_t s) {
+// Mod-6 patterns: word W of class c's table, group x: bit b = 1 iff
+// 6g + c has no factor in the group, g = (32w + b) mod period.
+__device__ __forceinline__ uint32_t wheel6_group_prime(int x, int j) {
+  return x == 0 ? (j == 0 ? 5 : j == 1 ? 7 : j == 2 ? 11 : j == 3 ? 13 : 0) : wheel_group_prime(x, j);
+}
+
+__global__ void wheel6_init_kernel(uint32_t* wheel6) {
+  const uint32_t W = blockIdx.x * blockDim.x + threadIdx.x;
+  if (W >= kWheel6Words) return;
+  const int cls5 = W >= kWheel6ClassWords;
+  const uint32_t wc = W - (cls5 ? kWheel6ClassWords : 0);
+  int x = 0;
+  while (x + 1 < kWheel6Groups && wc >= wheel6_group_offset(x + 1)) ++x;
+  const uint32_t P = wheel6_period(x);
+  const uint32_t w = wc - wheel6_group_offset(x);
+  const uint32_t c = cls5 ? 5 : 1;
+  uint32_t v = 0;
+  for (int b = 0; b < 32; ++b) {
+    const uint32_t g = (32u * w + b) % P;
+    bool keep = true;
+    for (int j = 0; j < 5; ++j) {
+      const uint32_t p = wheel6_group_prime(x, j);
+      if (p && (6ull * g + c) % p == 0) keep = false;
+    }
+    if (keep) v |= 1u << b;
+  }
+  wheel6[W] = v;
+}
+
+cudaError_t launch_wheel_init(uint32_t* wheel, uint32_t* wheel6, cudaStream_t s) {
   wheel_init_kernel<<<(kWheelWords + 255) / 256, 256, 0, s>>>(wheel);
+  wheel6_init_kernel<<<(kWheel6Words + 255) / 256, 256, 0, s>>>(wheel6);
   return cudaGetLastError();
 }
 
@@ -164,7 +194,7 @@ __global__ void __launch_bounds__(1024) compact_scan_kernel(uint32_t* blocks, ui
 
 __global__ void __launch_bounds__(kCompactWords) compact_write_kernel(
     const uint32_t* bits, uint64_t nwords, uint64_t q_lo, const uint32_t* blocks,
-    uint32_t* primes, uint64_t* magic, uint64_t prefix, uint64_t cap) {
+    uint32_t* primes, uint64_t* magic, uint2* a15, uint64_t prefix, uint64_t cap) {
   const uint64_t w = (uint64_t)blockIdx.x * kCompactWords + threadIdx.x;
   uint32_t v = w < nwords ? bits[w] : 0;
   const uint32_t c = __popc(v);
@@ -196,30 +226,39 @@ __global__ void __launch_bounds__(kCompactWords) compact_write_kernel(
     if (pos < cap) {
       primes[pos] = (uint32_t)q;
       magic[pos] = ~0ull / q;
+      // class offsets of the mod-6 sieve: a1 = -1/6, a5 = -5/6 (mod q)
+      uint2 a = make_uint2(0, 0);
+      if (q >= 5) {
+        const uint64_t inv6 = (q % 6 == 1) ? (5 * q + 1) / 6 : (q + 1) / 6;
+        const uint64_t a1 = q - inv6;
+        a = make_uint2((uint32_t)a1, (uint32_t)((5 * a1) % q));
+      }
+      a15[pos] = a;
     }
     ++pos;
   }
 }
 
-__global__ void put_two_kernel(uint32_t* primes, uint64_t* magic) {
+__global__ void put_two_kernel(uint32_t* primes, uint64_t* magic, uint2* a15) {
   primes[0] = 2;
   magic[0] = ~0ull / 2;
+  a15[0] = make_uint2(0, 0);
 }
 
 cudaError_t launch_compact_primes(const uint32_t* bits, uint64_t nbits, uint64_t q_lo,
-                                  uint32_t* primes, uint64_t* magic, uint64_t prefix,
+                                  uint32_t* primes, uint64_t* magic, uint2* a15, uint64_t prefix,
                                   uint64_t cap, unsigned long long* d_total,
                                   uint32_t* scratch_blocks, uint32_t nblocks_cap,
                                   cudaStream_t s) {
   const uint64_t nwords = (nbits + 31) / 32;
   const uint32_t nblocks = (uint32_t)compact_scratch_blocks(nbits);
   if (nblocks > nblocks_cap) return cudaErrorInvalidValue;
-  if (prefix == 1) put_two_kernel<<<1, 1, 0, s>>>(primes, magic);
+  if (prefix == 1) put_two_kernel<<<1, 1, 0, s>>>(primes, magic, a15);
   if (nblocks == 0) return cudaGetLastError();
   compact_count_kernel<<<nblocks, kCompactWords, 0, s>>>(bits, nwords, scratch_blocks);
   compact_scan_kernel<<<1, 1024, 0, s>>>(scratch_blocks, nblocks, prefix, d_total);
   compact_write_kernel<<<nblocks, kCompactWords, 0, s>>>(bits, nwords, q_lo, scratch_blocks,
-                                                         primes, magic, prefix, cap);
+                                                         primes, magic, a15, prefix, cap);
   return cudaGetLastError();
 }
 

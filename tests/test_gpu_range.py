@@ -80,7 +80,10 @@ def test_chunk_sizes(ctx, oracle, primes, chunk):
 def test_halo_sizes_and_phase2_path(ctx, oracle, primes, halo):
     r, mp = run_and_check(ctx, oracle, primes, 10**9 + 2, 1 << 16, halo=halo)
     if halo == 128:
-        assert r.result["queued"] == int((mp > 127).sum()) > 0
+        # the window search covers the primes p <= H - 13 (every q = n - p
+        # then lies inside the chunk's q-window); larger minimal p go to
+        # the device Phase 2
+        assert r.result["queued"] == int((mp > halo - 13).sum()) > 0
 
 
 def test_bounds_force_failures(ctx, oracle, primes):
