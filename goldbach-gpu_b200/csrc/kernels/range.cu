@@ -124,6 +124,7 @@ __global__ void __launch_bounds__(kRangeThreads, 2) range6_kernel(const __grid_c
       cx.maxp = 0;
       cx.psum = 0;
       cx.next_task = 0;
+      cx.maxk = 0;
     }
     for (uint32_t i = tid; i < kSmemHistBins; i += kRangeThreads) HIST[i] = 0;
     __syncthreads();
@@ -156,8 +157,9 @@ __global__ void __launch_bounds__(kRangeThreads, 2) range6_kernel(const __grid_c
         const uint32_t d = (uint32_t)((2 * ri - (int)amod + 6) % 6);
         cx.n[ri] = A + d;
         cx.M[ri] = last >= A + d ? (uint32_t)((last - A - d) / 6 + 1) : 0u;
-        cx.X[ri][0] = a6 + d - 1;
-        cx.X[ri][1] = a6 + d - 5;
+        // K = (X - (p mod 6)) / 6 with X = n_rho - c - 6 G0 (exact)
+        cx.K[ri][0] = (a6 + d - 1 - e6_pmod(ri, 0)) / 6;
+        cx.K[ri][1] = (a6 + d - 5 - e6_pmod(ri, 1)) / 6;
       }
     }
     const uint32_t nbits = s.halo / 6 + cnt / 3 + 96;

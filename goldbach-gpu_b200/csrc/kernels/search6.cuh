@@ -14,9 +14,13 @@
 //     t = m + (X - p) / 6,   X = n_rho - c - 6 G0   (an exact division),
 // uniform per warp, so 32 n are tested against one p with one funnel shift.
 //
-// The lockstep phase reads the first kLockSteps6 entries of each class
-// sequence from shared memory, packed as
-//     p (bits 0-16) | k (bits 17-30, index in the prime table) | q-class 5 (bit 31)
+// Within a class, p mod 6 is fixed by q's class (rho 0: p = 1 <-> q in class
+// 5; rho 2, 4: the q-class of p = 3 and of the rest differ), so with
+// u = floor(p / 6) the offset is one subtraction, t = m + K - u, with
+// K = (X - (p mod 6)) / 6 per (class, q-class).  The lockstep phase reads the
+// first kLockSteps6 entries of each class sequence from shared memory,
+// packed as
+//     u (bits 0-14) | k (bits 15-28, index in the prime table) | q-class 5 (bit 31)
 // (p < 2^17 and k < 2^14 hold for every halo <= 2^17); the few n left after
 // it continue one at a time over the global prime table.
 #pragma once
@@ -28,7 +32,7 @@
 
 namespace gb {
 
-constexpr uint32_t kE6PBits = 17;
+constexpr uint32_t kE6UBits = 15;
 constexpr uint32_t kLockSteps6 = 96;  // lockstep entries of each class sequence
 
 // Per-CTA search context in shared memory: the class tables' lengths (fixed
@@ -46,11 +50,12 @@ struct Ctx6 {
   uint64_t unit;      // segment
   uint64_t n[3];      // n_rho: first n of each class
   uint32_t M[3];      // n of each class
-  uint32_t X[3][2];   // X for q-class 1 and 5
+  uint32_t K[3][2];   // K for q-class 1 and 5
   // the chunk's accounting (zeroed before the search)
   uint32_t fb, maxp;
   unsigned long long psum;
   uint32_t next_task;  // the chunk's next warp task
+  uint32_t maxk;       // 1 + largest prime index in the chunk's histogram
 };
 
 // Shared-memory pointers of a CTA's search (known to be shared memory at
@@ -64,25 +69,27 @@ struct Smem6 {
   const uint32_t* E4;
 };
 
-__device__ __forceinline__ uint32_t e6_p(uint32_t e) { return e & ((1u << kE6PBits) - 1); }
-__device__ __forceinline__ uint32_t e6_k(uint32_t e) { return (e >> kE6PBits) & 0x3fffu; }
-// (X - p) / 6 for X - p a multiple of 6: halve, then multiply by 1/3 mod 2^32
-__device__ __forceinline__ uint32_t e6_off(uint32_t X, uint32_t p) {
-  return ((X - p) >> 1) * 0xAAAAAAABu;
-}
+__device__ __forceinline__ uint32_t e6_u(uint32_t e) { return e & ((1u << kE6UBits) - 1); }
+__device__ __forceinline__ uint32_t e6_k(uint32_t e) { return (e >> kE6UBits) & 0x3fffu; }
 __device__ __forceinline__ uint32_t div6(uint32_t p) { return __umulhi(p, 715827883u); }
+// p mod 6 of the entries of class ri whose q lies in class 5 (q5 = 1) or 1
+__device__ __forceinline__ uint32_t e6_pmod(int ri, uint32_t q5) {
+  return ri == 0 ? (q5 ? 1 : 5) : ri == 1 ? (q5 ? 3 : 1) : (q5 ? 5 : 3);
+}
 
 // Scalar finish of one n = n_rho + 6m (ri = rho / 2) after the lockstep
 // entries of its class: the window primes from cx->kend[ri] on, filtered
-// to the class.  Returns the minimal p found here (0 if none) in the low 32
-// bits and 1 in bit 32 when it counts as a fallback.
+// to the class.  A minimal p of prime index below kSmemHistBins goes to the
+// shared histogram (the flush derives the chunk's figures from it) and 0 is
+// returned; otherwise the minimal p (0 if none) in the low 32 bits and 1 in
+// bit 32 when the n counts as a fallback.
 template <bool MINP>
 __device__ __noinline__ uint64_t tail_one6(const SearchParams& s, const Ctx6* cx, int ri,
                                            uint32_t m) {
   const uint64_t n = cx->n[ri] + 6ull * m;
   const uint64_t half = n >> 1;
   const uint64_t idx = cx->base_idx + ((n - cx->A) >> 1);
-  const uint32_t X1 = cx->X[ri][0], X5 = cx->X[ri][1];
+  const uint32_t K1 = cx->K[ri][0], K5 = cx->K[ri][1];
   bool past_half = false;
   for (uint32_t k = cx->kend[ri]; k < s.nsearch; ++k) {
     const uint32_t p = s.primes[k];
@@ -93,17 +100,17 @@ __device__ __noinline__ uint64_t tail_one6(const SearchParams& s, const Ctx6* cx
     const bool p1 = p - 6 * div6(p) == 1;  // p >= 5 here
     if ((ri == 1 && !p1) || (ri == 2 && p1)) continue;  // q = n - p divisible by 3
     const bool q5 = ri == 0 ? p1 : ri == 2;
-    const uint32_t bit = e6_off(q5 ? X5 : X1, p) + m;
+    const uint32_t bit = (q5 ? K5 : K1) - div6(p) + m;
     const uint32_t w = (q5 ? cx->Q5 : cx->Q1)[bit >> 5];
     if ((w >> (bit & 31)) & 1u) {
-      if (k < kSmemHistBins) {
-        atomicAdd(&cx->HIST[k], 1u);
-      } else {
-        const uint32_t bin = k < GB_HIST_BINS - 1 ? k : GB_HIST_BINS - 1;
-        if (s.hist) atomicAdd(&s.hist[bin], 1ull);
-        if (s.unit_hist) atomicAdd(&s.unit_hist[cx->unit * GB_HIST_BINS + bin], 1ull);
-      }
       if (MINP) s.minp[idx] = p;
+      if (k < kSmemHistBins) {  // accounted from the histogram at the flush
+        atomicAdd(&cx->HIST[k], 1u);
+        return 0;
+      }
+      const uint32_t bin = k < GB_HIST_BINS - 1 ? k : GB_HIST_BINS - 1;
+      if (s.hist) atomicAdd(&s.hist[bin], 1ull);
+      if (s.unit_hist) atomicAdd(&s.unit_hist[cx->unit * GB_HIST_BINS + bin], 1ull);
       return (uint64_t)p | ((uint64_t)(k >= s.kfb) << 32);
     }
   }
@@ -161,7 +168,7 @@ template <bool MINP, int WT>
 __device__ __forceinline__ uint32_t step6(const SearchParams& s, uint32_t (&U)[WT],
                                           const uint32_t (&lo)[WT], const uint32_t (&hi)[WT],
                                           uint32_t sh, uint32_t p, uint32_t wbase,
-                                          uint64_t ibase) {
+                                          uint64_t ibase) {  // p: MINP only
   uint32_t cnt = 0;
 #pragma unroll
   for (int i = 0; i < WT; ++i) {
@@ -208,14 +215,13 @@ __device__ __forceinline__ void search_task6(const SearchParams& s, const Smem6&
   // n = 4 (p = 2) and n = 6 (p = 3, q = 3): the classes hold no q = 2, 3
   if (task == 0 && lane == 0 && (U[0] & 1u) && ((ri == 2 && n0 == 4) || (ri == 0 && n0 == 6))) {
     U[0] &= ~1u;
-    const uint32_t p = ri == 2 ? 2 : 3;
-    record_found_k(s, sm.HIST, p - 2, p, cx->unit, acc);
-    if (MINP) s.minp[cx->base_idx + ((n0 - cx->A) >> 1)] = p;
+    atomicAdd(&sm.HIST[ri == 2 ? 0 : 1], 1u);
+    if (MINP) s.minp[cx->base_idx + ((n0 - cx->A) >> 1)] = ri == 2 ? 2 : 3;
   }
   // (selected, not indexed: a run-time index would put sm on the stack)
   const uint32_t* __restrict__ E = ri == 0 ? sm.E0 : ri == 1 ? sm.E2 : sm.E4;
   const uint32_t steps = cx->len[ri];
-  const uint32_t X1 = cx->X[ri][0], X5 = cx->X[ri][1];
+  const uint32_t K1 = cx->K[ri][0], K5 = cx->K[ri][1];
   const uint64_t ibase = cx->base_idx + ((n0 - cx->A) >> 1);
   Cache6<kWT> ca;
   for (uint32_t pos = 0; pos < steps; ++pos) {
@@ -226,20 +232,14 @@ __device__ __forceinline__ void search_task6(const SearchParams& s, const Smem6&
       if (!__any_sync(0xffffffffu, any)) break;
     }
     const uint32_t e = E[pos];
-    const uint32_t p = e6_p(e);
     const uint32_t q5 = e >> 31;
-    const uint32_t off = e6_off(q5 ? X5 : X1, p);
+    const uint32_t off = (q5 ? K5 : K1) - e6_u(e);
     const uint32_t wo = off >> 5;
     ca.at(q5 ? sm.Q5 : sm.Q1, wo, wo | (q5 << 31), wbase);
+    const uint32_t p = MINP ? 6 * e6_u(e) + e6_pmod(ri, q5) : 0;
     uint32_t cnt = step6<MINP, kWT>(s, U, ca.lo, ca.hi, off & 31, p, wbase, ibase);
     cnt = __reduce_add_sync(0xffffffffu, cnt);
-    if (lane == 0 && cnt) {
-      const uint32_t k = e6_k(e);
-      atomicAdd(&sm.HIST[k], cnt);
-      if (k >= s.kfb) acc.fb += cnt;
-      if (p > acc.maxp) acc.maxp = p;
-      acc.psum += (uint64_t)cnt * p;
-    }
+    if (lane == 0 && cnt) atomicAdd(&sm.HIST[e6_k(e)], cnt);
   }
   // the n left after the lockstep entries, one at a time
 #pragma unroll
@@ -279,28 +279,41 @@ __device__ __forceinline__ void search_chunk6(const SearchParams& s, const Smem6
     else if (task < t2 + t4) search_task6<MINP>(s, sm, cx, 2, task - t2, acc);
     else search_task6<MINP>(s, sm, cx, 0, task - t2 - t4, acc);
   }
-  if (acc.fb) atomicAdd(&cx->fb, acc.fb);
-  if (acc.maxp) atomicMax(&cx->maxp, acc.maxp);
-  if (acc.psum) atomicAdd(&cx->psum, (unsigned long long)acc.psum);
+  // the chunk's figures: tails beyond the shared histogram (acc), plus
+  // fallbacks, largest and summed minimal p read off the histogram
   __syncthreads();
   const uint64_t unit = cx->unit;
-  if (s.hist || s.unit_hist) {
-    for (uint32_t k = tid; k < kSmemHistBins; k += NT) {
-      const uint32_t v = sm.HIST[k];
-      if (v) {
-        if (s.hist) atomicAdd(&s.hist[k], (unsigned long long)v);
-        if (s.unit_hist) atomicAdd(&s.unit_hist[unit * GB_HIST_BINS + k], (unsigned long long)v);
-      }
+  uint32_t fbh = acc.fb, maxk = 0;
+  unsigned long long ps = acc.psum;
+  for (uint32_t k = tid; k < kSmemHistBins; k += NT) {
+    const uint32_t v = sm.HIST[k];
+    if (v) {
+      if (s.hist) atomicAdd(&s.hist[k], (unsigned long long)v);
+      if (s.unit_hist) atomicAdd(&s.unit_hist[unit * GB_HIST_BINS + k], (unsigned long long)v);
+      if (k >= s.kfb) fbh += v;
+      if (s.unit_psum) ps += (unsigned long long)v * s.primes[k];
+      maxk = k + 1;
     }
   }
+  fbh = __reduce_add_sync(0xffffffffu, fbh);
+  maxk = __reduce_max_sync(0xffffffffu, maxk);
+  if (lane == 0) {
+    if (fbh) atomicAdd(&cx->fb, fbh);
+    if (maxk) atomicMax(&cx->maxk, maxk);
+  }
+  if (acc.maxp) atomicMax(&cx->maxp, acc.maxp);
+  if (ps) atomicAdd(&cx->psum, ps);
+  __syncthreads();
   if (tid == 0) {
+    const uint32_t hp = cx->maxk ? s.primes[cx->maxk - 1] : 0;
+    const uint32_t maxp = hp > cx->maxp ? hp : cx->maxp;
     if (cx->fb) {
       atomicAdd(&s.ctr[kCtrFallbacks], (unsigned long long)cx->fb);
       if (s.unit_fallbacks) atomicAdd(&s.unit_fallbacks[unit], cx->fb);
     }
-    if (cx->maxp) {
-      atomicMax(&s.ctr[kCtrMaxP], (unsigned long long)cx->maxp);
-      if (s.unit_maxp) atomicMax(&s.unit_maxp[unit], (unsigned long long)cx->maxp);
+    if (maxp) {
+      atomicMax(&s.ctr[kCtrMaxP], (unsigned long long)maxp);
+      if (s.unit_maxp) atomicMax(&s.unit_maxp[unit], (unsigned long long)maxp);
     }
     if (cx->psum && s.unit_psum) atomicAdd(&s.unit_psum[unit], cx->psum);
   }
@@ -323,7 +336,7 @@ __device__ __forceinline__ void load_tables6(const SearchParams& s, Ctx6* cx, ui
       const bool in = k < ns;
       const uint32_t p = in ? s.primes[k] : 0;
       const bool p1 = p - 6 * div6(p) == 1;
-      const uint32_t e = p | (k << kE6PBits);
+      const uint32_t e = div6(p) | (k << kE6UBits);
       const uint32_t lt = (1u << lane) - 1;
       // E0: class bit = q in class 5 = (p = 1 mod 6)
       if (in && k - 2 < L) E0[k - 2] = e | ((uint32_t)p1 << 31);
@@ -344,8 +357,8 @@ __device__ __forceinline__ void load_tables6(const SearchParams& s, Ctx6* cx, ui
       n4 = min(L, n4 + __popc(b4));
     }
     if (lane == 0) {
-      E2[0] = 3u | (1u << kE6PBits) | (1u << 31);  // rho 2: q = n - 3 in class 5
-      E4[0] = 3u | (1u << kE6PBits);               // rho 4: q = n - 3 in class 1
+      E2[0] = (1u << kE6UBits) | (1u << 31);  // rho 2: p = 3 (u = 0), q in class 5
+      E4[0] = 1u << kE6UBits;                 // rho 4: p = 3, q in class 1
       cx->len[0] = n0;
       cx->len[1] = n2;
       cx->len[2] = n4;
