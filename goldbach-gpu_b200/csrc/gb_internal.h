@@ -69,6 +69,8 @@ struct RangeArgs {
   int layout6;
   const uint32_t* wheel6;  // kWheel6Words
   const uint2* a15;
+  uint2* surv;             // survivor lists: 3 per CTA of surv_cap entries each
+  uint32_t surv_cap;       // >= words of one class bitset
 };
 
 struct SieveArgs {

@@ -97,13 +97,29 @@ gb_status ws_init(gb_ctx* c, Workspace& w, uint32_t queue_cap) {
   return GB_OK;
 }
 
+gb_status ws_scratch(gb_ctx* c, Workspace& w, size_t bytes, void** p) {
+  if (bytes > w.scratch_bytes) {
+    dev_free(c, w.scratch);
+    w.scratch = nullptr;
+    w.scratch_bytes = 0;
+    gb_status st = dev_alloc(c, &w.scratch, bytes, &w.err);
+    if (st != GB_OK) return st;
+    w.scratch_bytes = bytes;
+  }
+  *p = w.scratch;
+  return GB_OK;
+}
+
 void ws_free(gb_ctx* c, Workspace& w) {
   dev_free(c, w.ctr);
   dev_free(c, w.hist);
   dev_free(c, w.queue);
+  dev_free(c, w.scratch);
   w.ctr = nullptr;
   w.hist = nullptr;
   w.queue = nullptr;
+  w.scratch = nullptr;
+  w.scratch_bytes = 0;
   for (cudaEvent_t* e : {&w.ev0, &w.ev1, &w.ek0, &w.ek1})
     if (*e) {
       cudaEventDestroy(*e);
@@ -393,6 +409,12 @@ gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint
   if (bps < 1) bps = 1;
   uint64_t grid = (uint64_t)c->sm_count * bps;
   if (a.total_items < grid) grid = std::max<uint64_t>(1, a.total_items);
+  if (a.layout6 && a.total_items) {  // survivor lists of the two-phase search
+    a.surv_cap = a.nbw;
+    void* p = nullptr;
+    if ((st = ws_scratch(c, w, (size_t)grid * 3 * a.surv_cap * sizeof(uint2), &p)) != GB_OK) return st;
+    a.surv = (uint2*)p;
+  }
   if (a.total_items) {
     chk(cudaEventRecord(w.ek0, s));
     chk(launch_range(a, (int)grid, s));
@@ -567,10 +589,13 @@ uint64_t gb_estimate_device_bytes(const gb_config* cfg) {
   if (cfg && cfg->max_n) want = std::max<uint64_t>(want, isqrt_u64(cfg->max_n) + 2);
   want = std::max<uint64_t>(want, 1ull << 22);
   const uint64_t np = pi_upper(want);
-  // primes + reciprocals, the build bitset and scan blocks, wheel, counters,
-  // histogram and the Phase-2 queue
-  return np * 20 + want / 16 + (want / 65536 + 1) * 4 + kWheelWords * 4 + kCtrCount * 8 +
-         GB_HIST_BINS * 8 + (1ull << 20) * sizeof(QEntry);
+  // primes + reciprocals + class offsets, the build bitset and scan
+  // blocks, wheels, counters, histogram, the Phase-2 queue, and the range
+  // search's survivor lists (2 CTAs on up to 160 SMs, 3 lists of up to
+  // 2^20/96 + 512 words)
+  return np * 20 + want / 16 + (want / 65536 + 1) * 4 + (kWheelWords + kWheel6Words) * 4 +
+         kCtrCount * 8 + GB_HIST_BINS * 8 + (1ull << 20) * sizeof(QEntry) +
+         320ull * 3 * ((1u << 20) / 96 + 512) * 8;
 }
 
 gb_status gb_create(int device, const gb_config* cfg, gb_ctx** out) {

@@ -45,6 +45,8 @@ struct Workspace {
   QEntry* queue = nullptr;
   uint32_t queue_cap = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ek0 = nullptr, ek1 = nullptr;
+  void* scratch = nullptr;  // per-call kernel scratch, grown on demand
+  size_t scratch_bytes = 0;
   std::string err;
 };
 
@@ -92,6 +94,8 @@ gb_status dev_alloc(gb_ctx* c, void** p, size_t bytes, std::string* err = nullpt
 void dev_free(gb_ctx* c, void* p);
 gb_status ws_init(gb_ctx* c, Workspace& w, uint32_t queue_cap);
 void ws_free(gb_ctx* c, Workspace& w);
+// The workspace's scratch buffer, grown to at least `bytes`.
+gb_status ws_scratch(gb_ctx* c, Workspace& w, size_t bytes, void** p);
 gb_status ensure_primes(gb_ctx* c, Workspace& w, uint64_t limit);
 // number of primes <= x in the resident table (x <= primes_limit)
 gb_status count_le(gb_ctx* c, Workspace& w, uint64_t x, uint64_t* out);

@@ -95,27 +95,19 @@ __device__ __forceinline__ int64_t window_g0(uint64_t A, uint32_t H) {
 
 template <bool MINP>
 __global__ void __launch_bounds__(kRangeThreads, 2) range6_kernel(const __grid_constant__ RangeArgs a) {
-  extern __shared__ uint32_t smem[];
   const SearchParams& s = a.s;
-  uint32_t* pat6 = smem;
-  uint32_t* Q1 = pat6 + kWheel6Words;
-  uint32_t* Q5 = Q1 + a.nbw;
-  uint32_t* HIST = Q5 + a.nbw;
-  uint32_t* E0 = HIST + kSmemHistBins;
-  uint32_t* E2 = E0 + kLockSteps6;
-  uint32_t* E4 = E2 + kLockSteps6;
-  __shared__ Ctx6 cx;
   __shared__ unsigned long long s_item;
   const int tid = threadIdx.x;
-
+  Ctx6& cx = g_cx6;
+  uint32_t* pat6 = smem6_pat();
   for (uint32_t i = tid; i < kWheel6Words; i += kRangeThreads) pat6[i] = a.wheel6[i];
-  if (tid == 0) {
-    cx.Q1 = Q1;
-    cx.Q5 = Q5;
-    cx.HIST = HIST;
-  }
-  load_tables6(s, &cx, E0, E2, E4);
-  const Smem6 sm{Q1, Q5, HIST, E0, E2, E4};
+  if (tid == 0) cx.nbw = a.nbw;
+  __syncthreads();
+  load_tables6(s);
+  uint32_t* Q1 = smem6_q(0);
+  uint32_t* Q5 = smem6_q(1);
+  uint32_t* HIST = smem6_hist();
+  uint2* surv = a.surv + (size_t)blockIdx.x * 3 * a.surv_cap;
 
   for (;;) {
     if (tid == 0) {
@@ -124,6 +116,8 @@ __global__ void __launch_bounds__(kRangeThreads, 2) range6_kernel(const __grid_c
       cx.maxp = 0;
       cx.psum = 0;
       cx.next_task = 0;
+      cx.next_task2 = 0;
+      cx.scnt[0] = cx.scnt[1] = cx.scnt[2] = 0;
       cx.maxk = 0;
     }
     for (uint32_t i = tid; i < kSmemHistBins; i += kRangeThreads) HIST[i] = 0;
@@ -165,7 +159,7 @@ __global__ void __launch_bounds__(kRangeThreads, 2) range6_kernel(const __grid_c
     const uint32_t nbits = s.halo / 6 + cnt / 3 + 96;
     sieve_window6<kRangeThreads>(Q1, Q5, a.nbw, nbits, G0, A + 2ull * cnt, pat6, s.primes,
                                  a.magic, a.a15, a.nsieve, a.kcoop);
-    search_chunk6<MINP, kRangeThreads>(s, sm, &cx);
+    search_chunk6<MINP, kRangeThreads>(s, surv, a.surv_cap);
   }
 }
 
@@ -231,7 +225,7 @@ __global__ void __launch_bounds__(kFallbackThreads) fallback_kernel(const __grid
 // ---------------------------------------------------------------------------
 size_t range_smem_bytes(const RangeArgs& a) {
   if (a.layout6)
-    return (size_t)(kWheel6Words + 2 * a.nbw + kSmemHistBins + 3 * kLockSteps6) * sizeof(uint32_t);
+    return range6_smem_words(a.nbw) * sizeof(uint32_t);
   return (size_t)(kWheelWords + a.nbw + kSmemHistBins) * sizeof(uint32_t) +
          (size_t)((a.s.nsearch + 1) & ~1u) * sizeof(uint16_t);
 }

@@ -26,6 +26,7 @@
 #pragma once
 #include <cstdint>
 
+#include "../gb_device.cuh"
 #include "../gb_internal.h"
 #include "gb/gb.h"
 #include "search.cuh"
@@ -34,14 +35,16 @@ namespace gb {
 
 constexpr uint32_t kE6UBits = 15;
 constexpr uint32_t kLockSteps6 = 96;  // lockstep entries of each class sequence
+// Phase A runs every task through the first kSurvSteps6 entries; the words
+// still holding an unresolved n (about 1 in 6 near 1e12) go to a per-class
+// survivor list, and phase B runs them, densely packed, through the rest.
+constexpr uint32_t kSurvSteps6 = 40;
 
-// Per-CTA search context in shared memory: the class tables' lengths (fixed
-// for the kernel) and the current chunk (written by one thread before the
-// search).  The generic pointers serve the per-n tail.
+// Per-CTA search context (static shared memory): the class tables' lengths
+// (fixed for the kernel) and the current chunk (written by one thread
+// before the sieve).
 struct Ctx6 {
-  const uint32_t* Q1;
-  const uint32_t* Q5;
-  uint32_t* HIST;
+  uint32_t nbw;      // words of each class bitset
   uint32_t len[3];   // lockstep entries of each class (<= kLockSteps6)
   uint32_t kend[3];  // prime index after each class's last lockstep entry
   // the chunk
@@ -51,23 +54,31 @@ struct Ctx6 {
   uint64_t n[3];      // n_rho: first n of each class
   uint32_t M[3];      // n of each class
   uint32_t K[3][2];   // K for q-class 1 and 5
-  // the chunk's accounting (zeroed before the search)
-  uint32_t fb, maxp;
-  unsigned long long psum;
-  uint32_t next_task;  // the chunk's next warp task
-  uint32_t maxk;       // 1 + largest prime index in the chunk's histogram
+  // the chunk's accounting (zeroed before the sieve)
+  uint32_t fb, maxp;        // from the per-n tails (the histogram gives the rest)
+  unsigned long long psum;  // likewise
+  uint32_t next_task;       // the chunk's next phase-A warp task
+  uint32_t next_task2;      // the chunk's next phase-B warp task
+  uint32_t scnt[3];         // survivor words of each class
+  uint32_t maxk;            // 1 + largest prime index in the chunk's histogram
 };
 
-// Shared-memory pointers of a CTA's search (known to be shared memory at
-// the call site, so the compiler addresses them with 32-bit offsets).
-struct Smem6 {
-  const uint32_t* Q1;
-  const uint32_t* Q5;
-  uint32_t* HIST;
-  const uint32_t* E0;
-  const uint32_t* E2;
-  const uint32_t* E4;
-};
+__shared__ Ctx6 g_cx6;
+// dynamic shared memory of range6_kernel:
+//   class wheel patterns | Q1 | Q5 (nbw words each) | HIST | E0 | E2 | E4
+extern __shared__ uint32_t g_smem6[];
+
+__device__ __forceinline__ uint32_t* smem6_pat() { return g_smem6; }
+__device__ __forceinline__ uint32_t* smem6_q(uint32_t cls5) {
+  return g_smem6 + kWheel6Words + (cls5 ? g_cx6.nbw : 0u);
+}
+__device__ __forceinline__ uint32_t* smem6_hist() { return g_smem6 + kWheel6Words + 2 * g_cx6.nbw; }
+__device__ __forceinline__ uint32_t* smem6_etab(int ri) {
+  return smem6_hist() + kSmemHistBins + ri * kLockSteps6;
+}
+__host__ __device__ constexpr size_t range6_smem_words(uint32_t nbw) {
+  return kWheel6Words + 2 * (size_t)nbw + kSmemHistBins + 3 * kLockSteps6;
+}
 
 __device__ __forceinline__ uint32_t e6_u(uint32_t e) { return e & ((1u << kE6UBits) - 1); }
 __device__ __forceinline__ uint32_t e6_k(uint32_t e) { return (e >> kE6UBits) & 0x3fffu; }
@@ -78,20 +89,19 @@ __device__ __forceinline__ uint32_t e6_pmod(int ri, uint32_t q5) {
 }
 
 // Scalar finish of one n = n_rho + 6m (ri = rho / 2) after the lockstep
-// entries of its class: the window primes from cx->kend[ri] on, filtered
-// to the class.  A minimal p of prime index below kSmemHistBins goes to the
-// shared histogram (the flush derives the chunk's figures from it) and 0 is
-// returned; otherwise the minimal p (0 if none) in the low 32 bits and 1 in
-// bit 32 when the n counts as a fallback.
+// entries of its class: the window primes from kend[ri] on, filtered to the
+// class.  A minimal p of prime index below kSmemHistBins goes to the shared
+// histogram (the flush derives the chunk's figures from it); larger ones,
+// Phase-2 queueing and failures are accounted here.
 template <bool MINP>
-__device__ __noinline__ uint64_t tail_one6(const SearchParams& s, const Ctx6* cx, int ri,
-                                           uint32_t m) {
-  const uint64_t n = cx->n[ri] + 6ull * m;
+__device__ __noinline__ void tail_one6(const SearchParams& s, int ri, uint32_t m) {
+  const Ctx6& cx = g_cx6;
+  const uint64_t n = cx.n[ri] + 6ull * m;
   const uint64_t half = n >> 1;
-  const uint64_t idx = cx->base_idx + ((n - cx->A) >> 1);
-  const uint32_t K1 = cx->K[ri][0], K5 = cx->K[ri][1];
+  const uint64_t idx = cx.base_idx + ((n - cx.A) >> 1);
+  const uint32_t K1 = cx.K[ri][0], K5 = cx.K[ri][1];
   bool past_half = false;
-  for (uint32_t k = cx->kend[ri]; k < s.nsearch; ++k) {
+  for (uint32_t k = cx.kend[ri]; k < s.nsearch; ++k) {
     const uint32_t p = s.primes[k];
     if (p > half) {
       past_half = true;
@@ -99,19 +109,22 @@ __device__ __noinline__ uint64_t tail_one6(const SearchParams& s, const Ctx6* cx
     }
     const bool p1 = p - 6 * div6(p) == 1;  // p >= 5 here
     if ((ri == 1 && !p1) || (ri == 2 && p1)) continue;  // q = n - p divisible by 3
-    const bool q5 = ri == 0 ? p1 : ri == 2;
+    const uint32_t q5 = ri == 0 ? p1 : ri == 2;
     const uint32_t bit = (q5 ? K5 : K1) - div6(p) + m;
-    const uint32_t w = (q5 ? cx->Q5 : cx->Q1)[bit >> 5];
+    const uint32_t w = smem6_q(q5)[bit >> 5];
     if ((w >> (bit & 31)) & 1u) {
       if (MINP) s.minp[idx] = p;
-      if (k < kSmemHistBins) {  // accounted from the histogram at the flush
-        atomicAdd(&cx->HIST[k], 1u);
-        return 0;
+      if (k < kSmemHistBins) {
+        atomicAdd(&smem6_hist()[k], 1u);
+        return;
       }
       const uint32_t bin = k < GB_HIST_BINS - 1 ? k : GB_HIST_BINS - 1;
       if (s.hist) atomicAdd(&s.hist[bin], 1ull);
-      if (s.unit_hist) atomicAdd(&s.unit_hist[cx->unit * GB_HIST_BINS + bin], 1ull);
-      return (uint64_t)p | ((uint64_t)(k >= s.kfb) << 32);
+      if (s.unit_hist) atomicAdd(&s.unit_hist[cx.unit * GB_HIST_BINS + bin], 1ull);
+      if (k >= s.kfb) atomicAdd(&g_cx6.fb, 1u);
+      atomicMax(&g_cx6.maxp, p);
+      atomicAdd(&g_cx6.psum, (unsigned long long)p);
+      return;
     }
   }
   // every window prime p <= n/2 tried: the Phase-2 queue or a failure
@@ -119,41 +132,42 @@ __device__ __noinline__ uint64_t tail_one6(const SearchParams& s, const Ctx6* cx
   if (past_half || s.nsearch >= s.nprimes || s.primes[s.nsearch] > lim) {
     atomicAdd(&s.ctr[kCtrFailures], 1ull);
     atomicMin(&s.ctr[kCtrFirstFail], (unsigned long long)n);
-    if (s.unit_failures) atomicAdd(&s.unit_failures[cx->unit], 1u);
+    if (s.unit_failures) atomicAdd(&s.unit_failures[cx.unit], 1u);
     if (s.vbits) atomicAnd(&s.vbits[idx >> 5], ~(1u << (idx & 31)));
-    return 1ull << 32;
+    atomicAdd(&g_cx6.fb, 1u);  // a failure counts as a fallback
+    return;
   }
   const unsigned long long slot = atomicAdd(&s.ctr[kCtrQueue], 1ull);
   if (slot < s.queue_cap) {
     s.queue[slot].n = n;
     s.queue[slot].idx = idx;
-    s.queue[slot].unit = cx->unit;
+    s.queue[slot].unit = cx.unit;
   } else {
     s.ctr[kCtrQueueOvf] = 1ull;
   }
-  return 0;
 }
 
-// Window words of one class bitset for the WT U words of a lane, reloaded
-// only when the key (the word offset, with the class in bit 31) changes.
+// Window words of one class bitset for the WT U words of a lane (word
+// indices W), reloaded only when the key (the word offset, with the class
+// in bit 31) changes.
 template <int WT>
 struct Cache6 {
   uint32_t lo[WT], hi[WT];
   uint32_t key = 0xffffffffu;
   __device__ __forceinline__ void at(const uint32_t* __restrict__ Q, uint32_t wo, uint32_t k,
-                                     uint32_t wbase) {
+                                     const uint32_t (&W)[WT]) {
     if (k == key) return;
     if (k + 1 == key) {
 #pragma unroll
       for (int i = 0; i < WT; ++i) {
         hi[i] = lo[i];
-        lo[i] = Q[wo + wbase + 32 * i];
+        lo[i] = Q[wo + W[i]];
       }
     } else {
 #pragma unroll
       for (int i = 0; i < WT; ++i) {
-        lo[i] = Q[wo + wbase + 32 * i];
-        hi[i] = Q[wo + wbase + 32 * i + 1];
+        lo[i] = Q[wo + W[i]];
+        hi[i] = Q[wo + W[i] + 1];
       }
     }
     key = k;
@@ -167,7 +181,7 @@ struct Cache6 {
 template <bool MINP, int WT>
 __device__ __forceinline__ uint32_t step6(const SearchParams& s, uint32_t (&U)[WT],
                                           const uint32_t (&lo)[WT], const uint32_t (&hi)[WT],
-                                          uint32_t sh, uint32_t p, uint32_t wbase,
+                                          uint32_t sh, uint32_t p, const uint32_t (&W)[WT],
                                           uint64_t ibase) {  // p: MINP only
   uint32_t cnt = 0;
 #pragma unroll
@@ -177,7 +191,7 @@ __device__ __forceinline__ uint32_t step6(const SearchParams& s, uint32_t (&U)[W
     cnt += __popc(h);
     if (MINP) {
       if (h) {
-        const uint64_t m0 = 32ull * (wbase + 32 * i);
+        const uint64_t m0 = 32ull * W[i];
         while (h) {
           const int b = __ffs(h) - 1;
           h &= h - 1;
@@ -189,43 +203,66 @@ __device__ __forceinline__ uint32_t step6(const SearchParams& s, uint32_t (&U)[W
   return cnt;
 }
 
-// One warp task: class ri (rho = 2 ri), words [task*kTaskWords, +kTaskWords)
-// of that class; lane l owns words task*kTaskWords + l + 32i.  Lockstep over
-// the class sequence with one window-word cache keyed by (offset, class).
-template <bool MINP>
-__device__ __forceinline__ void search_task6(const SearchParams& s, const Smem6& sm,
-                                             const Ctx6* cx, int ri, uint32_t task,
-                                             LaneAcc& acc) {
+// One warp task of class ri (rho = 2 ri).  Phase A (PB false): words
+// [task*kTaskWords, +kTaskWords) of the class, lane l owning words
+// task*kTaskWords + l + 32i, through the first kSurvSteps6 entries; words
+// still unresolved are appended to the class's survivor list surv (at most
+// one entry per word, so it cannot overflow).  Phase B: entries
+// [task*kTaskWords, +kTaskWords) of that list through the remaining
+// entries.  Lockstep over the class sequence with one window-word cache
+// keyed by (offset, class); the n left at the end are finished one by one.
+// Not inlined: the task gets the whole register file of the thread (the
+// chunk loop around it keeps nothing live across the call).
+template <bool MINP, bool PB>
+__device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_t task,
+                                          uint2* __restrict__ surv) {
+  const Ctx6& cx = g_cx6;
   const int lane = threadIdx.x & 31;
-  const uint32_t M = cx->M[ri];
-  const uint32_t nuw = (M + 31) >> 5;
-  const uint32_t wbase = task * kTaskWords + lane;
-  const uint64_t n0 = cx->n[ri];
-  uint32_t U[kWT];
+  const uint64_t n0 = cx.n[ri];
+  uint32_t U[kWT], W[kWT];
+  if (!PB) {
+    const uint32_t M = cx.M[ri];
+    const uint32_t nuw = (M + 31) >> 5;
+    const uint32_t wbase = task * kTaskWords + lane;
 #pragma unroll
-  for (int i = 0; i < kWT; ++i) {
-    const uint32_t w = wbase + 32 * i;
-    uint32_t mk = 0;
-    if (w < nuw) {
-      const uint32_t rem = M - 32 * w;
-      mk = rem >= 32 ? 0xffffffffu : ((1u << rem) - 1);
+    for (int i = 0; i < kWT; ++i) {
+      const uint32_t w = wbase + 32 * i;
+      uint32_t mk = 0;
+      if (w < nuw) {
+        const uint32_t rem = M - 32 * w;
+        mk = rem >= 32 ? 0xffffffffu : ((1u << rem) - 1);
+      }
+      U[i] = mk;
+      W[i] = w;
     }
-    U[i] = mk;
+    // n = 4 (p = 2) and n = 6 (p = 3, q = 3): the classes hold no q = 2, 3
+    if (task == 0 && lane == 0 && (U[0] & 1u) && ((ri == 2 && n0 == 4) || (ri == 0 && n0 == 6))) {
+      U[0] &= ~1u;
+      atomicAdd(&smem6_hist()[ri == 2 ? 0 : 1], 1u);
+      if (MINP) s.minp[cx.base_idx + ((n0 - cx.A) >> 1)] = ri == 2 ? 2 : 3;
+    }
+  } else {
+    const uint32_t cnt = cx.scnt[ri];
+#pragma unroll
+    for (int i = 0; i < kWT; ++i) {
+      const uint32_t j = task * kTaskWords + lane + 32 * i;
+      const uint2 v = j < cnt ? surv[j] : make_uint2(0u, 0u);
+      W[i] = v.x;
+      U[i] = v.y;
+    }
   }
-  // n = 4 (p = 2) and n = 6 (p = 3, q = 3): the classes hold no q = 2, 3
-  if (task == 0 && lane == 0 && (U[0] & 1u) && ((ri == 2 && n0 == 4) || (ri == 0 && n0 == 6))) {
-    U[0] &= ~1u;
-    atomicAdd(&sm.HIST[ri == 2 ? 0 : 1], 1u);
-    if (MINP) s.minp[cx->base_idx + ((n0 - cx->A) >> 1)] = ri == 2 ? 2 : 3;
-  }
-  // (selected, not indexed: a run-time index would put sm on the stack)
-  const uint32_t* __restrict__ E = ri == 0 ? sm.E0 : ri == 1 ? sm.E2 : sm.E4;
-  const uint32_t steps = cx->len[ri];
-  const uint32_t K1 = cx->K[ri][0], K5 = cx->K[ri][1];
-  const uint64_t ibase = cx->base_idx + ((n0 - cx->A) >> 1);
+  const uint32_t* __restrict__ E = smem6_etab(ri);
+  const uint32_t* __restrict__ Q1 = smem6_q(0);
+  const uint32_t* __restrict__ Q5 = smem6_q(1);
+  uint32_t* HIST = smem6_hist();
+  const uint32_t len = cx.len[ri];
+  const uint32_t pos0 = PB ? kSurvSteps6 : 0;
+  const uint32_t pend = PB ? len : (len < kSurvSteps6 ? len : kSurvSteps6);
+  const uint32_t K1 = cx.K[ri][0], K5 = cx.K[ri][1];
+  const uint64_t ibase = cx.base_idx + ((n0 - cx.A) >> 1);
   Cache6<kWT> ca;
-  for (uint32_t pos = 0; pos < steps; ++pos) {
-    if ((pos & 7) == 0) {
+  for (uint32_t pos = pos0; pos < pend; ++pos) {
+    if (((pos - pos0) & 7) == 0) {
       uint32_t any = 0;
 #pragma unroll
       for (int i = 0; i < kWT; ++i) any |= U[i];
@@ -235,11 +272,26 @@ __device__ __forceinline__ void search_task6(const SearchParams& s, const Smem6&
     const uint32_t q5 = e >> 31;
     const uint32_t off = (q5 ? K5 : K1) - e6_u(e);
     const uint32_t wo = off >> 5;
-    ca.at(q5 ? sm.Q5 : sm.Q1, wo, wo | (q5 << 31), wbase);
+    ca.at(q5 ? Q5 : Q1, wo, wo | (q5 << 31), W);
     const uint32_t p = MINP ? 6 * e6_u(e) + e6_pmod(ri, q5) : 0;
-    uint32_t cnt = step6<MINP, kWT>(s, U, ca.lo, ca.hi, off & 31, p, wbase, ibase);
+    uint32_t cnt = step6<MINP, kWT>(s, U, ca.lo, ca.hi, off & 31, p, W, ibase);
     cnt = __reduce_add_sync(0xffffffffu, cnt);
-    if (lane == 0 && cnt) atomicAdd(&sm.HIST[e6_k(e)], cnt);
+    if (lane == 0 && cnt) atomicAdd(&HIST[e6_k(e)], cnt);
+  }
+  if (!PB && len > kSurvSteps6) {
+    // unresolved words continue in phase B
+    const uint32_t lt = (1u << lane) - 1;
+#pragma unroll
+    for (int i = 0; i < kWT; ++i) {
+      const uint32_t alive = __ballot_sync(0xffffffffu, U[i] != 0);
+      if (alive) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&g_cx6.scnt[ri], (uint32_t)__popc(alive));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (U[i]) surv[base + __popc(alive & lt)] = make_uint2(W[i], U[i]);
+        U[i] = 0;
+      }
+    }
   }
   // the n left after the lockstep entries, one at a time
 #pragma unroll
@@ -248,45 +300,60 @@ __device__ __forceinline__ void search_task6(const SearchParams& s, const Smem6&
     while (u) {
       const int b = __ffs(u) - 1;
       u &= u - 1;
-      const uint64_t r = tail_one6<MINP>(s, cx, ri, 32 * (wbase + 32 * i) + b);
-      const uint32_t p = (uint32_t)r;
-      acc.fb += (uint32_t)(r >> 32);
-      if (p > acc.maxp) acc.maxp = p;
-      acc.psum += p;
+      tail_one6<MINP>(s, ri, 32 * W[i] + b);
     }
   }
 }
 
 // Whole-chunk search by the CTA plus the flush of its accounting (same
-// contract as search_chunk in search.cuh).  sm.HIST, cx's fb, maxp and psum
-// and cx->next_task must be zero before the call.  Warps take tasks from a
-// shared counter, classes 2 and 4 (the longer sequences) first.  Ends with
-// __syncthreads().
+// contract as search_chunk in search.cuh).  The histogram, g_cx6's fb,
+// maxp, psum, maxk, scnt and task counters must be zero before the call.
+// Warps take tasks from shared counters, classes 2 and 4 first; surv holds
+// the CTA's three survivor lists of surv_cap entries (>= words of a class).
+// Ends with __syncthreads().
 template <bool MINP, int NT>
-__device__ __forceinline__ void search_chunk6(const SearchParams& s, const Smem6& sm, Ctx6* cx) {
+__device__ __forceinline__ void search_chunk6(const SearchParams& s, uint2* surv,
+                                              uint32_t surv_cap) {
   const int tid = threadIdx.x;
   const int lane = tid & 31;
-  const uint32_t t0 = (((cx->M[0] + 31) >> 5) + kTaskWords - 1) / kTaskWords;
-  const uint32_t t2 = (((cx->M[1] + 31) >> 5) + kTaskWords - 1) / kTaskWords;
-  const uint32_t t4 = (((cx->M[2] + 31) >> 5) + kTaskWords - 1) / kTaskWords;
-  LaneAcc acc{0, 0, 0};
-  for (;;) {
-    uint32_t task = 0;
-    if (lane == 0) task = atomicAdd(&cx->next_task, 1u);
-    task = __shfl_sync(0xffffffffu, task, 0);
-    if (task >= t0 + t2 + t4) break;
-    if (task < t2) search_task6<MINP>(s, sm, cx, 1, task, acc);
-    else if (task < t2 + t4) search_task6<MINP>(s, sm, cx, 2, task - t2, acc);
-    else search_task6<MINP>(s, sm, cx, 0, task - t2 - t4, acc);
+  {
+    const uint32_t t0 = (((g_cx6.M[0] + 31) >> 5) + kTaskWords - 1) / kTaskWords;
+    const uint32_t t2 = (((g_cx6.M[1] + 31) >> 5) + kTaskWords - 1) / kTaskWords;
+    const uint32_t t4 = (((g_cx6.M[2] + 31) >> 5) + kTaskWords - 1) / kTaskWords;
+    for (;;) {  // phase A
+      uint32_t task = 0;
+      if (lane == 0) task = atomicAdd(&g_cx6.next_task, 1u);
+      task = __shfl_sync(0xffffffffu, task, 0);
+      if (task >= t0 + t2 + t4) break;
+      const int ri = task < t2 ? 1 : task < t2 + t4 ? 2 : 0;
+      const uint32_t t = ri == 1 ? task : ri == 2 ? task - t2 : task - t2 - t4;
+      search_task6<MINP, false>(s, ri, t, surv + ri * surv_cap);
+    }
   }
-  // the chunk's figures: tails beyond the shared histogram (acc), plus
-  // fallbacks, largest and summed minimal p read off the histogram
   __syncthreads();
-  const uint64_t unit = cx->unit;
-  uint32_t fbh = acc.fb, maxk = 0;
-  unsigned long long ps = acc.psum;
+  {
+    const uint32_t b0 = (g_cx6.scnt[0] + kTaskWords - 1) / kTaskWords;
+    const uint32_t b2 = (g_cx6.scnt[1] + kTaskWords - 1) / kTaskWords;
+    const uint32_t b4 = (g_cx6.scnt[2] + kTaskWords - 1) / kTaskWords;
+    for (;;) {  // phase B
+      uint32_t task = 0;
+      if (lane == 0) task = atomicAdd(&g_cx6.next_task2, 1u);
+      task = __shfl_sync(0xffffffffu, task, 0);
+      if (task >= b0 + b2 + b4) break;
+      const int ri = task < b2 ? 1 : task < b2 + b4 ? 2 : 0;
+      const uint32_t t = ri == 1 ? task : ri == 2 ? task - b2 : task - b2 - b4;
+      search_task6<MINP, true>(s, ri, t, surv + ri * surv_cap);
+    }
+  }
+  // the chunk's figures: the tails' (in g_cx6) plus fallbacks, largest and
+  // summed minimal p read off the histogram
+  __syncthreads();
+  const uint32_t* HIST = smem6_hist();
+  const uint64_t unit = g_cx6.unit;
+  uint32_t fbh = 0, maxk = 0;
+  unsigned long long ps = 0;
   for (uint32_t k = tid; k < kSmemHistBins; k += NT) {
-    const uint32_t v = sm.HIST[k];
+    const uint32_t v = HIST[k];
     if (v) {
       if (s.hist) atomicAdd(&s.hist[k], (unsigned long long)v);
       if (s.unit_hist) atomicAdd(&s.unit_hist[unit * GB_HIST_BINS + k], (unsigned long long)v);
@@ -298,24 +365,23 @@ __device__ __forceinline__ void search_chunk6(const SearchParams& s, const Smem6
   fbh = __reduce_add_sync(0xffffffffu, fbh);
   maxk = __reduce_max_sync(0xffffffffu, maxk);
   if (lane == 0) {
-    if (fbh) atomicAdd(&cx->fb, fbh);
-    if (maxk) atomicMax(&cx->maxk, maxk);
+    if (fbh) atomicAdd(&g_cx6.fb, fbh);
+    if (maxk) atomicMax(&g_cx6.maxk, maxk);
   }
-  if (acc.maxp) atomicMax(&cx->maxp, acc.maxp);
-  if (ps) atomicAdd(&cx->psum, ps);
+  if (ps) atomicAdd(&g_cx6.psum, ps);
   __syncthreads();
   if (tid == 0) {
-    const uint32_t hp = cx->maxk ? s.primes[cx->maxk - 1] : 0;
-    const uint32_t maxp = hp > cx->maxp ? hp : cx->maxp;
-    if (cx->fb) {
-      atomicAdd(&s.ctr[kCtrFallbacks], (unsigned long long)cx->fb);
-      if (s.unit_fallbacks) atomicAdd(&s.unit_fallbacks[unit], cx->fb);
+    const uint32_t hp = g_cx6.maxk ? s.primes[g_cx6.maxk - 1] : 0;
+    const uint32_t maxp = hp > g_cx6.maxp ? hp : g_cx6.maxp;
+    if (g_cx6.fb) {
+      atomicAdd(&s.ctr[kCtrFallbacks], (unsigned long long)g_cx6.fb);
+      if (s.unit_fallbacks) atomicAdd(&s.unit_fallbacks[unit], g_cx6.fb);
     }
     if (maxp) {
       atomicMax(&s.ctr[kCtrMaxP], (unsigned long long)maxp);
       if (s.unit_maxp) atomicMax(&s.unit_maxp[unit], (unsigned long long)maxp);
     }
-    if (cx->psum && s.unit_psum) atomicAdd(&s.unit_psum[unit], cx->psum);
+    if (g_cx6.psum && s.unit_psum) atomicAdd(&s.unit_psum[unit], g_cx6.psum);
   }
   __syncthreads();
 }
@@ -323,10 +389,13 @@ __device__ __forceinline__ void search_chunk6(const SearchParams& s, const Smem6
 // Fills the CTA's lockstep tables (kLockSteps6 entries each at most) from
 // primes[2 .. nsearch):
 //   E0: every p >= 5;  E2: 3, then p = 1 (mod 6);  E4: 3, then p = 5 (mod 6);
-// and sets cx->len / cx->kend.  One warp; ends with __syncthreads().
-__device__ __forceinline__ void load_tables6(const SearchParams& s, Ctx6* cx, uint32_t* E0,
-                                             uint32_t* E2, uint32_t* E4) {
+// and sets g_cx6.len / kend.  g_cx6.nbw must be set.  One warp; ends with
+// __syncthreads().
+__device__ __forceinline__ void load_tables6(const SearchParams& s) {
   if (threadIdx.x < 32) {
+    uint32_t* E0 = smem6_etab(0);
+    uint32_t* E2 = smem6_etab(1);
+    uint32_t* E4 = smem6_etab(2);
     const int lane = threadIdx.x;
     const uint32_t ns = s.nsearch;
     constexpr uint32_t L = kLockSteps6;
@@ -359,12 +428,12 @@ __device__ __forceinline__ void load_tables6(const SearchParams& s, Ctx6* cx, ui
     if (lane == 0) {
       E2[0] = (1u << kE6UBits) | (1u << 31);  // rho 2: p = 3 (u = 0), q in class 5
       E4[0] = 1u << kE6UBits;                 // rho 4: p = 3, q in class 1
-      cx->len[0] = n0;
-      cx->len[1] = n2;
-      cx->len[2] = n4;
-      cx->kend[0] = k0end;
-      cx->kend[1] = k2end;
-      cx->kend[2] = k4end;
+      g_cx6.len[0] = n0;
+      g_cx6.len[1] = n2;
+      g_cx6.len[2] = n4;
+      g_cx6.kend[0] = k0end;
+      g_cx6.kend[1] = k2end;
+      g_cx6.kend[2] = k4end;
     }
   }
   __syncthreads();
