@@ -35,15 +35,32 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 METRIC = "even n verified/s to 1e12 on 1 B200, batched vs plain; p50/p99 query latency"
 UNIT = "even n/s"
 
-# Algorithmic work per even n of [4, 1e12]: ideal
-# word-parallel search steps (the largest minimal-p index of each 32-n word,
-# averaged over the range with the oracle) at 5 ALU ops each, the wheel fill
-# (7 pattern ANDs of 2 ops per 32 odd q), and Eratosthenes marks of the
-# primes 71..sqrt(n) per odd q of the q-windows.
-SEARCH_STEPS_PER_N = 1.6286
-SEARCH_OPS_PER_STEP = 5
-WHEEL_OPS_PER_BIT = 14 / 32
+# Algorithmic work of the range workload, in layout-independent units (the
+# odd-only problem statement):
+#  * search: sum over n of pi(p_min(n)) scalar (n, p) tests, 32 per word
+#    operation of 5 ALU ops (shift, and, xor, popc, add); 14.85 tests per n
+#    is the oracle's mean over [4, 1e12] (32 strata of 2^16 n);
+#  * sieve: wheel pattern words for the primes 3..67 (7 ANDs of 2 ops per 32
+#    odd q) and Eratosthenes marks of the primes 71..sqrt(n) per odd q of
+#    each chunk's q-window (sum of 1/p = 1.1225 for sqrt(n) = 1e6), one
+#    shared-memory atomic each;
+#  * one first-multiple reduction (8 ALU ops) per sieving prime per chunk.
+SEARCH_TESTS_PER_N = 14.85
+SEARCH_OPS_PER_WORD = 5
+WHEEL_OPS_PER_ODD_Q = 14 / 32
 MARKS_PER_ODD_Q = 1.1225
+OPS_PER_OFFSET = 8
+
+
+def sieving_primes(limit):
+    """pi(isqrt(limit)): the primes that sieve each chunk's q-window."""
+    r = math.isqrt(limit)
+    sieve = bytearray([1]) * (r + 1)
+    sieve[0:2] = b"\0\0"
+    for i in range(2, math.isqrt(r) + 1):
+        if sieve[i]:
+            sieve[i * i::i] = bytearray(len(range(i * i, r + 1, i)))
+    return sum(sieve)
 
 
 def load_gb():
@@ -300,6 +317,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--limit", type=int, default=10**12)
+    ap.add_argument("--count", type=int, default=0,
+                    help="time only the top COUNT even n below --limit (default: all of [4, limit])")
     ap.add_argument("--seg-size", type=int, default=1 << 27)
     ap.add_argument("--chunk", type=int, default=0)
     ap.add_argument("--halo", type=int, default=0)
@@ -326,7 +345,8 @@ def main():
     multi = load_multi()
     ctx = gb.Context(local, max_n=args.limit)
     stream = torch.cuda.Stream()
-    start, limit = 4, args.limit - (args.limit & 1)
+    limit = args.limit - (args.limit & 1)
+    start = max(4, limit - 2 * (args.count - 1)) if args.count else 4
     total = (limit - start) // 2 + 1
     nseg = gb.load().gb_num_segments(start, limit, args.seg_size)
     dev = torch.device("cuda", local)
@@ -411,27 +431,30 @@ def main():
     e2e_value = total / (ems / 1000)
     d2h = 4096 * 8 + nseg * 8 + 8 * 8
 
-    # roofline of range_kernel (the dominant kernel, ~100% of the device
+    # roofline of range6_kernel (the dominant kernel, ~100% of the device
     # time): algorithmic integer work of this rank's share over its average
     # launch time, against ALU and shared-memory-atomic peaks measured here.
     halo = args.halo or 32768
-    chunk = args.chunk or (1 << 19)
+    chunk = args.chunk or (1 << 20)
     n_mine = multi.shard_even_count(total, args.seg_size, rank, world)
-    bits_per_n = 1 + (halo // 2) / chunk
-    alu_ops = n_mine * (SEARCH_STEPS_PER_N * SEARCH_OPS_PER_STEP + WHEEL_OPS_PER_BIT * bits_per_n)
-    marks = n_mine * MARKS_PER_ODD_Q * bits_per_n
+    odd_q_per_n = 1 + (halo // 2) / chunk
+    chunks = math.ceil(n_mine / chunk)
+    offsets = chunks * sieving_primes(limit)
+    alu_ops = (n_mine * (SEARCH_TESTS_PER_N / 32 * SEARCH_OPS_PER_WORD
+                         + WHEEL_OPS_PER_ODD_Q * odd_q_per_n) + offsets * OPS_PER_OFFSET)
+    marks = n_mine * MARKS_PER_ODD_Q * odd_q_per_n
     alu_peak, atom_peak = ctx.probe_peaks()
     k_s = statistics.mean(kms) / 1000
     sol_s = alu_ops / alu_peak + marks / atom_peak
     achieved = (alu_ops + marks * alu_peak / atom_peak) / k_s
     hbm, hbm_kind = hbm_peak()
-    hbm_bytes = 2 * n_mine * bits_per_n / 8  # the q-bitset, had it gone through HBM
+    hbm_bytes = 2 * n_mine * odd_q_per_n / 8  # the q-bitset, had it gone through HBM
     res0 = results[-1]
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"range [4, {limit}] (every even n)", "seg_size": args.seg_size,
+        "config": {"workload": f"range [{start}, {limit}] (every even n)", "seg_size": args.seg_size,
                    "chunk_evens": chunk, "halo": halo, "p_small": 10**6, "phase2_limit": 10**8,
                    "l2": "flushed (512 MB write) between steps",
                    "parallelism": f"segments sharded over {world} GPU(s)"},
@@ -440,10 +463,11 @@ def main():
         "roofline": {
             "bound": "int", "achieved": achieved / 1e12, "peak": alu_peak / 1e12, "unit": "Top/s",
             "frac": achieved / alu_peak, "traffic": None,
-            "kernel": "range_kernel", "kernel_ms": k_s * 1e3,
+            "kernel": "range6_kernel", "kernel_ms": k_s * 1e3,
             "peak_source": "measured in-process: gb_probe_peaks (32-bit ALU ops/s; shared-memory atomicAnd/s)",
             "smem_atomic_peak": atom_peak, "alu_ops_per_launch": alu_ops,
-            "smem_marks_per_launch": marks, "speed_of_light_ms": sol_s * 1e3,
+            "smem_marks_per_launch": marks, "offsets_per_launch": offsets,
+            "speed_of_light_ms": sol_s * 1e3,
             "hbm": {"achieved": hbm_bytes / k_s / 1e9, "peak": hbm, "unit": "GB/s",
                     "frac": hbm_bytes / k_s / 1e9 / hbm, "peak_source": hbm_kind,
                     "note": "q-bitset bytes a staged design would move; the fused kernel keeps them on chip"}},

@@ -130,6 +130,7 @@ size_t compact_scratch_blocks(uint64_t nbits);
 
 // kernels/range.cu
 size_t range_smem_bytes(const RangeArgs& a);
+uint32_t range6_words(uint32_t halo, uint32_t chunk_evens);
 int range_max_blocks_per_sm(const RangeArgs& a);
 cudaError_t launch_range(const RangeArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_fallback(const SearchParams& s, int grid, cudaStream_t st);

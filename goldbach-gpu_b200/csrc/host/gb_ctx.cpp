@@ -322,9 +322,9 @@ gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint
   a.layout6 = kRangeLayout6;
   uint64_t search_top, window_bits;
   if (kRangeLayout6) {
-    // two class bitsets of H/6 + NE/3 bits (plus the funnel over-read of the
-    // last warp task); primes p <= H - 13 keep every q = n - p in the window
-    a.nbw = (H / 6 + 96) / 32 + 1 + (((NE / 3 + 2) / 32 + 256) & ~255u) + 4;
+    // two class bitsets of H/6 + NE/3 bits (plus the over-read of the last
+    // warp task); primes p <= H - 13 keep every q = n - p in the window
+    a.nbw = range6_words(H, NE);
     search_top = std::min<uint64_t>(H - 13, p_lim);
     window_bits = H / 6 + NE / 3;
   } else {

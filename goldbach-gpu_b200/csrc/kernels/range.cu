@@ -223,6 +223,17 @@ __global__ void __launch_bounds__(kFallbackThreads) fallback_kernel(const __grid
 }
 
 // ---------------------------------------------------------------------------
+// Words of each class bitset: the largest q-window word offset a search
+// step reads (H/6 + 96 bits), plus the U words of a class rounded up to
+// whole warp tasks (the last task reads past the chunk's words), plus the
+// second word of each funnel shift and a little slack.
+uint32_t range6_words(uint32_t halo, uint32_t chunk_evens) {
+  const uint32_t off_words = (halo / 6 + 96) / 32 + 1;
+  const uint32_t class_words = (chunk_evens / 3 + 2 + 31) / 32;
+  const uint32_t tasks = (class_words + kTaskWords6 - 1) / kTaskWords6;
+  return off_words + tasks * kTaskWords6 + 4;
+}
+
 size_t range_smem_bytes(const RangeArgs& a) {
   if (a.layout6)
     return range6_smem_words(a.nbw) * sizeof(uint32_t);

@@ -25,6 +25,7 @@
 // it continue one at a time over the global prime table.
 #pragma once
 #include <cstdint>
+#include <type_traits>
 
 #include "../gb_device.cuh"
 #include "../gb_internal.h"
@@ -34,11 +35,13 @@
 namespace gb {
 
 constexpr uint32_t kE6UBits = 15;
-constexpr uint32_t kLockSteps6 = 96;  // lockstep entries of each class sequence
+constexpr uint32_t kLockSteps6 = 128; // lockstep entries of each class sequence
 // Phase A runs every task through the first kSurvSteps6 entries; the words
 // still holding an unresolved n (about 1 in 6 near 1e12) go to a per-class
 // survivor list, and phase B runs them, densely packed, through the rest.
 constexpr uint32_t kSurvSteps6 = 40;
+constexpr int kWT6 = 7;                      // U words per lane per warp task
+constexpr uint32_t kTaskWords6 = 32 * kWT6;  // words per warp task
 
 // Per-CTA search context (static shared memory): the class tables' lengths
 // (fixed for the kernel) and the current chunk (written by one thread
@@ -147,6 +150,18 @@ __device__ __noinline__ void tail_one6(const SearchParams& s, int ri, uint32_t m
   }
 }
 
+// Word indices of a lane's U words: strided from a base word (phase A) or
+// listed (phase B).
+struct WordsStrided {
+  uint32_t base;
+  __device__ __forceinline__ uint32_t operator[](int i) const { return base + 32 * i; }
+};
+template <int WT>
+struct WordsListed {
+  uint32_t w[WT];
+  __device__ __forceinline__ uint32_t operator[](int i) const { return w[i]; }
+};
+
 // Window words of one class bitset for the WT U words of a lane (word
 // indices W), reloaded only when the key (the word offset, with the class
 // in bit 31) changes.
@@ -154,8 +169,9 @@ template <int WT>
 struct Cache6 {
   uint32_t lo[WT], hi[WT];
   uint32_t key = 0xffffffffu;
+  template <typename Words>
   __device__ __forceinline__ void at(const uint32_t* __restrict__ Q, uint32_t wo, uint32_t k,
-                                     const uint32_t (&W)[WT]) {
+                                     const Words& W) {
     if (k == key) return;
     if (k + 1 == key) {
 #pragma unroll
@@ -178,10 +194,10 @@ struct Cache6 {
 // for p > n/2 is needed (unlike the odd-only search): a partition n = p + q
 // with q < p would have been found at the smaller prime q, which is in the
 // same class sequence, and every q < 5 reads a cleared bit.
-template <bool MINP, int WT>
+template <bool MINP, int WT, typename Words>
 __device__ __forceinline__ uint32_t step6(const SearchParams& s, uint32_t (&U)[WT],
                                           const uint32_t (&lo)[WT], const uint32_t (&hi)[WT],
-                                          uint32_t sh, uint32_t p, const uint32_t (&W)[WT],
+                                          uint32_t sh, uint32_t p, const Words& W,
                                           uint64_t ibase) {  // p: MINP only
   uint32_t cnt = 0;
 #pragma unroll
@@ -204,36 +220,37 @@ __device__ __forceinline__ uint32_t step6(const SearchParams& s, uint32_t (&U)[W
 }
 
 // One warp task of class ri (rho = 2 ri).  Phase A (PB false): words
-// [task*kTaskWords, +kTaskWords) of the class, lane l owning words
-// task*kTaskWords + l + 32i, through the first kSurvSteps6 entries; words
+// [task*kTaskWords6, +kTaskWords6) of the class, lane l owning words
+// task*kTaskWords6 + l + 32i, through the first kSurvSteps6 entries; words
 // still unresolved are appended to the class's survivor list surv (at most
 // one entry per word, so it cannot overflow).  Phase B: entries
-// [task*kTaskWords, +kTaskWords) of that list through the remaining
-// entries.  Lockstep over the class sequence with one window-word cache
-// keyed by (offset, class); the n left at the end are finished one by one.
+// [task*kTaskWords6, +kTaskWords6) of that list through the remaining
+// entries, the words' unresolved bits written back in place.  Lockstep over
+// the class sequence with one window-word cache keyed by (offset, class).
 // Not inlined: the task gets the whole register file of the thread (the
-// chunk loop around it keeps nothing live across the call).
+// chunk loop around it keeps nothing live across the call), and it calls
+// nothing.
 template <bool MINP, bool PB>
 __device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_t task,
                                           uint2* __restrict__ surv) {
   const Ctx6& cx = g_cx6;
   const int lane = threadIdx.x & 31;
   const uint64_t n0 = cx.n[ri];
-  uint32_t U[kWT], W[kWT];
-  if (!PB) {
+  uint32_t U[kWT6];
+  typename std::conditional<PB, WordsListed<kWT6>, WordsStrided>::type W;
+  if constexpr (!PB) {
     const uint32_t M = cx.M[ri];
     const uint32_t nuw = (M + 31) >> 5;
-    const uint32_t wbase = task * kTaskWords + lane;
+    W.base = task * kTaskWords6 + lane;
 #pragma unroll
-    for (int i = 0; i < kWT; ++i) {
-      const uint32_t w = wbase + 32 * i;
+    for (int i = 0; i < kWT6; ++i) {
+      const uint32_t w = W[i];
       uint32_t mk = 0;
       if (w < nuw) {
         const uint32_t rem = M - 32 * w;
         mk = rem >= 32 ? 0xffffffffu : ((1u << rem) - 1);
       }
       U[i] = mk;
-      W[i] = w;
     }
     // n = 4 (p = 2) and n = 6 (p = 3, q = 3): the classes hold no q = 2, 3
     if (task == 0 && lane == 0 && (U[0] & 1u) && ((ri == 2 && n0 == 4) || (ri == 0 && n0 == 6))) {
@@ -244,10 +261,10 @@ __device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_
   } else {
     const uint32_t cnt = cx.scnt[ri];
 #pragma unroll
-    for (int i = 0; i < kWT; ++i) {
-      const uint32_t j = task * kTaskWords + lane + 32 * i;
+    for (int i = 0; i < kWT6; ++i) {
+      const uint32_t j = task * kTaskWords6 + lane + 32 * i;
       const uint2 v = j < cnt ? surv[j] : make_uint2(0u, 0u);
-      W[i] = v.x;
+      W.w[i] = v.x;
       U[i] = v.y;
     }
   }
@@ -260,12 +277,12 @@ __device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_
   const uint32_t pend = PB ? len : (len < kSurvSteps6 ? len : kSurvSteps6);
   const uint32_t K1 = cx.K[ri][0], K5 = cx.K[ri][1];
   const uint64_t ibase = cx.base_idx + ((n0 - cx.A) >> 1);
-  Cache6<kWT> ca;
+  Cache6<kWT6> ca;
   for (uint32_t pos = pos0; pos < pend; ++pos) {
     if (((pos - pos0) & 7) == 0) {
       uint32_t any = 0;
 #pragma unroll
-      for (int i = 0; i < kWT; ++i) any |= U[i];
+      for (int i = 0; i < kWT6; ++i) any |= U[i];
       if (!__any_sync(0xffffffffu, any)) break;
     }
     const uint32_t e = E[pos];
@@ -274,33 +291,30 @@ __device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_
     const uint32_t wo = off >> 5;
     ca.at(q5 ? Q5 : Q1, wo, wo | (q5 << 31), W);
     const uint32_t p = MINP ? 6 * e6_u(e) + e6_pmod(ri, q5) : 0;
-    uint32_t cnt = step6<MINP, kWT>(s, U, ca.lo, ca.hi, off & 31, p, W, ibase);
+    uint32_t cnt = step6<MINP, kWT6>(s, U, ca.lo, ca.hi, off & 31, p, W, ibase);
     cnt = __reduce_add_sync(0xffffffffu, cnt);
     if (lane == 0 && cnt) atomicAdd(&HIST[e6_k(e)], cnt);
   }
-  if (!PB && len > kSurvSteps6) {
+  if constexpr (!PB) {
     // unresolved words continue in phase B
     const uint32_t lt = (1u << lane) - 1;
 #pragma unroll
-    for (int i = 0; i < kWT; ++i) {
+    for (int i = 0; i < kWT6; ++i) {
       const uint32_t alive = __ballot_sync(0xffffffffu, U[i] != 0);
       if (alive) {
         uint32_t base = 0;
         if (lane == 0) base = atomicAdd(&g_cx6.scnt[ri], (uint32_t)__popc(alive));
         base = __shfl_sync(0xffffffffu, base, 0);
         if (U[i]) surv[base + __popc(alive & lt)] = make_uint2(W[i], U[i]);
-        U[i] = 0;
       }
     }
-  }
-  // the n left after the lockstep entries, one at a time
+  } else {
+    // what is left goes back in place for the per-n pass
+    const uint32_t cnt = cx.scnt[ri];
 #pragma unroll
-  for (int i = 0; i < kWT; ++i) {
-    uint32_t u = U[i];
-    while (u) {
-      const int b = __ffs(u) - 1;
-      u &= u - 1;
-      tail_one6<MINP>(s, ri, 32 * W[i] + b);
+    for (int i = 0; i < kWT6; ++i) {
+      const uint32_t j = task * kTaskWords6 + lane + 32 * i;
+      if (j < cnt) surv[j].y = U[i];
     }
   }
 }
@@ -317,9 +331,9 @@ __device__ __forceinline__ void search_chunk6(const SearchParams& s, uint2* surv
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   {
-    const uint32_t t0 = (((g_cx6.M[0] + 31) >> 5) + kTaskWords - 1) / kTaskWords;
-    const uint32_t t2 = (((g_cx6.M[1] + 31) >> 5) + kTaskWords - 1) / kTaskWords;
-    const uint32_t t4 = (((g_cx6.M[2] + 31) >> 5) + kTaskWords - 1) / kTaskWords;
+    const uint32_t t0 = (((g_cx6.M[0] + 31) >> 5) + kTaskWords6 - 1) / kTaskWords6;
+    const uint32_t t2 = (((g_cx6.M[1] + 31) >> 5) + kTaskWords6 - 1) / kTaskWords6;
+    const uint32_t t4 = (((g_cx6.M[2] + 31) >> 5) + kTaskWords6 - 1) / kTaskWords6;
     for (;;) {  // phase A
       uint32_t task = 0;
       if (lane == 0) task = atomicAdd(&g_cx6.next_task, 1u);
@@ -332,9 +346,9 @@ __device__ __forceinline__ void search_chunk6(const SearchParams& s, uint2* surv
   }
   __syncthreads();
   {
-    const uint32_t b0 = (g_cx6.scnt[0] + kTaskWords - 1) / kTaskWords;
-    const uint32_t b2 = (g_cx6.scnt[1] + kTaskWords - 1) / kTaskWords;
-    const uint32_t b4 = (g_cx6.scnt[2] + kTaskWords - 1) / kTaskWords;
+    const uint32_t b0 = (g_cx6.scnt[0] + kTaskWords6 - 1) / kTaskWords6;
+    const uint32_t b2 = (g_cx6.scnt[1] + kTaskWords6 - 1) / kTaskWords6;
+    const uint32_t b4 = (g_cx6.scnt[2] + kTaskWords6 - 1) / kTaskWords6;
     for (;;) {  // phase B
       uint32_t task = 0;
       if (lane == 0) task = atomicAdd(&g_cx6.next_task2, 1u);
@@ -343,6 +357,20 @@ __device__ __forceinline__ void search_chunk6(const SearchParams& s, uint2* surv
       const int ri = task < b2 ? 1 : task < b2 + b4 ? 2 : 0;
       const uint32_t t = ri == 1 ? task : ri == 2 ? task - b2 : task - b2 - b4;
       search_task6<MINP, true>(s, ri, t, surv + ri * surv_cap);
+    }
+  }
+  __syncthreads();
+  // phase C: the n still unresolved after every lockstep entry, one per thread
+  for (int ri = 0; ri < 3; ++ri) {
+    const uint2* L = surv + ri * surv_cap;
+    for (uint32_t j = tid; j < g_cx6.scnt[ri]; j += NT) {
+      const uint2 v = L[j];
+      uint32_t u = v.y;
+      while (u) {
+        const int b = __ffs(u) - 1;
+        u &= u - 1;
+        tail_one6<MINP>(s, ri, 32 * v.x + b);
+      }
     }
   }
   // the chunk's figures: the tails' (in g_cx6) plus fallbacks, largest and
