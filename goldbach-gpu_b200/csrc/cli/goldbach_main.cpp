@@ -9,7 +9,10 @@
 //
 // Additional flags: --chunk=N (even n per CTA window), --halo=N,
 // --phase2-limit=N, --device-mem-mb=N (device memory budget, used by the
-// VRAM guard), --json (one JSON summary line at the end).
+// VRAM guard), --json (one JSON summary line at the end), --journal=FILE
+// (resumable runs, journal.h) with --journal-segments=K (segments per
+// record) and --stop-after-batches=N (end the run after N new records, exit
+// code 3: the way tests interrupt a run).
 #include <atomic>
 #include <chrono>
 #include <cinttypes>
@@ -24,6 +27,7 @@
 #include <vector>
 
 #include "gb/gb.h"
+#include "journal.h"
 
 namespace {
 
@@ -48,6 +52,9 @@ void print_usage(const char* prog) {
             << "  --phase2-limit=N Phase 2 prime bound (default: 100,000,000)\n"
             << "  --device-mem-mb=N Device memory budget per GPU in MB\n"
             << "  --json           Print a JSON summary line\n"
+            << "  --journal=FILE   Record completed segments in FILE; rerun to resume\n"
+            << "  --journal-segments=K  Segments per journal record (default: about 2^36 n)\n"
+            << "  --stop-after-batches=N  Stop after N new journal records (exit code 3)\n"
             << "  -h, --help       Show this help message\n";
 }
 
@@ -69,6 +76,8 @@ int main(int argc, char** argv) {
   bool show_progress = false, json = false;
   uint64_t LIMIT = 0, SEG_SIZE = 10'000'000ULL, P_SMALL = 1'000'000ULL, START = 4;
   uint64_t chunk = 0, halo = 0, phase2 = 0, mem_mb = 0, batch = 100000;
+  std::string journal_path;
+  uint64_t journal_segs = 0, stop_after = 0;
   long requested_gpus = 1;
   std::vector<std::string> positional;
   try {
@@ -90,6 +99,9 @@ int main(int argc, char** argv) {
       if (arg.rfind("--halo=", 0) == 0) { halo = std::stoull(arg.substr(7)); continue; }
       if (arg.rfind("--phase2-limit=", 0) == 0) { phase2 = std::stoull(arg.substr(15)); continue; }
       if (arg.rfind("--device-mem-mb=", 0) == 0) { mem_mb = std::stoull(arg.substr(16)); continue; }
+      if (arg.rfind("--journal=", 0) == 0) { journal_path = arg.substr(10); continue; }
+      if (arg.rfind("--journal-segments=", 0) == 0) { journal_segs = std::stoull(arg.substr(19)); continue; }
+      if (arg.rfind("--stop-after-batches=", 0) == 0) { stop_after = std::stoull(arg.substr(21)); continue; }
       positional.push_back(arg);
     }
     if (positional.size() >= 1) LIMIT = std::stoull(positional[0]);
@@ -118,17 +130,6 @@ int main(int argc, char** argv) {
               << "    Recommended: P_SMALL >= 10^7 for numbers > 10^12\n"
               << "                 P_SMALL >= 10^8 for numbers > 10^18\n\n";
   }
-  const int device_count = gb_device_count();
-  if (device_count == 0) {
-    std::cerr << "No CUDA devices found.\n";
-    return 1;
-  }
-  if (requested_gpus > device_count) {
-    std::cerr << "Requested " << requested_gpus << " GPUs, but only " << device_count
-              << " available. Using " << device_count << ".\n";
-  }
-  const int use_gpus = (requested_gpus <= 0 || requested_gpus > device_count) ? device_count : (int)requested_gpus;
-
   // exact isqrt (src/goldbach.cu:637-646) and the small table bound (:648-649)
   uint64_t sqrt_limit = 0;
   {
@@ -142,6 +143,58 @@ int main(int argc, char** argv) {
   uint64_t small_high = std::max<uint64_t>(sqrt_limit + 1, P_SMALL);
   if (small_high % 2 == 0) small_high++;
   const uint64_t p2 = phase2 ? phase2 : GB_PHASE2_LIMIT_DEFAULT;
+  const uint64_t total = (LIMIT - START) / 2 + 1;
+  const uint64_t nseg = (total + SEG_SIZE - 1) / SEG_SIZE;
+
+  // The journal: what earlier runs of this command finished.
+  gbj::Journal journal;
+  Worker prior;  // journaled figures
+  std::vector<std::pair<uint64_t, uint64_t>> pending;
+  const bool journaling = !journal_path.empty();
+  if (journaling) {
+    std::string jerr;
+    if (!journal.open(journal_path, gbj::Key{START, LIMIT, SEG_SIZE, P_SMALL, p2}, &jerr)) {
+      std::cerr << "Error: " << jerr << "\n";
+      return 1;
+    }
+    uint64_t done_segs = 0;
+    for (const gbj::Record& r : journal.records()) {
+      done_segs += r.hi - r.lo;
+      prior.checked += r.checked;
+      prior.fallbacks += r.fallbacks;
+      prior.failures += r.failures;
+      prior.max_minp = std::max(prior.max_minp, r.max_minp);
+      if (r.first_fail && (!prior.first_fail || r.first_fail < prior.first_fail)) prior.first_fail = r.first_fail;
+    }
+    const uint64_t per = journal_segs ? journal_segs : std::max<uint64_t>(1, ((1ull << 36) + SEG_SIZE - 1) / SEG_SIZE);
+    pending = gbj::pending_batches(journal.records(), nseg, per);
+    if (!journal.records().empty())
+      std::cout << "Resuming from journal " << journal_path << ": " << done_segs << " of " << nseg
+                << " segments done, " << pending.size() << " batches to run\n";
+    if (pending.empty() || prior.failures) {  // nothing left for the GPU
+      if (prior.failures) {
+        std::cout << "\n[!] Goldbach FAILED at n = " << prior.first_fail << "\n";
+        return 1;
+      }
+      std::cout << "\n--- Verification Complete ---\n";
+      std::cout << "All even numbers from " << START << " up to " << LIMIT << " satisfy Goldbach. ✓\n";
+      std::cout << "Total computation time : 0 seconds\n";
+      std::cout << "Phase 2 fallbacks      : " << prior.fallbacks << "\n";
+      std::cout << "Max minimal p          : " << prior.max_minp << "\n";
+      return 0;
+    }
+  }
+
+  const int device_count = gb_device_count();
+  if (device_count == 0) {
+    std::cerr << "No CUDA devices found.\n";
+    return 1;
+  }
+  if (requested_gpus > device_count) {
+    std::cerr << "Requested " << requested_gpus << " GPUs, but only " << device_count
+              << " available. Using " << device_count << ".\n";
+  }
+  const int use_gpus = (requested_gpus <= 0 || requested_gpus > device_count) ? device_count : (int)requested_gpus;
 
   // VRAM guard (src/goldbach.cu:505-541) against what a context will hold;
   // --device-mem-mb caps the available memory.
@@ -182,7 +235,6 @@ int main(int argc, char** argv) {
   std::cout << "Initialization completed in "
             << std::chrono::duration<double, std::milli>(t1 - t0).count() << " ms.\n\n";
 
-  const uint64_t total = (LIMIT - START) / 2 + 1;
   std::cout << "--- Launching Multi-GPU Verifier ---\n";
   std::cout << "Checking range : [" << START << ", " << LIMIT << "]\n";
   std::cout << "Total numbers  : " << total << "\n\n";
@@ -191,18 +243,22 @@ int main(int argc, char** argv) {
   // Work is handed out in batches of whole segments so that segment numbers
   // stay those of the full range; GPU g takes batches g, g+G, ...  Without
   // --progress each GPU makes a single call over all its segments.
-  const uint64_t nseg = (total + SEG_SIZE - 1) / SEG_SIZE;
+  // With a journal the batches are the pending segment ranges, taken by
+  // the GPUs in turn, each recorded when it completes.
   uint64_t segs_per_batch = nseg;
   if (show_progress) segs_per_batch = std::max<uint64_t>(1, (nseg + 63) / 64);
-  const uint64_t nbatch = (nseg + segs_per_batch - 1) / segs_per_batch;
-  std::atomic<uint64_t> processed{0};
-  std::atomic<bool> stop{false};
+  const uint64_t nbatch = journaling ? pending.size() : (nseg + segs_per_batch - 1) / segs_per_batch;
+  std::atomic<uint64_t> processed{prior.checked};
+  std::atomic<uint64_t> next_batch{0}, recorded{0};
+  std::atomic<bool> stop{false}, interrupted{false};
+  std::mutex journal_mu;
   auto t_main = clk::now();
 
   auto run = [&](int g) {
     Worker& W = w[g];
-    const bool single_call = !show_progress;
-    for (uint64_t b = g; b < nbatch && !stop.load(); b += use_gpus) {
+    const bool single_call = !show_progress && !journaling;
+    for (uint64_t b = journaling ? next_batch++ : (uint64_t)g; b < nbatch && !stop.load();
+         b = journaling ? next_batch++ : b + use_gpus) {
       gb_range_opts o{};
       o.seg_size = SEG_SIZE;
       o.p_small = P_SMALL;
@@ -213,6 +269,9 @@ int main(int argc, char** argv) {
       if (single_call) {
         o.shard_index = g;
         o.shard_count = use_gpus;
+      } else if (journaling) {
+        a = START + 2 * SEG_SIZE * pending[b].first;
+        e = START + 2 * (std::min(total, SEG_SIZE * pending[b].second) - 1);
       } else {
         a = START + 2 * SEG_SIZE * segs_per_batch * b;
         const uint64_t last_idx = std::min(total, SEG_SIZE * segs_per_batch * (b + 1)) - 1;
@@ -237,6 +296,22 @@ int main(int argc, char** argv) {
         stop = true;
       }
       processed += r.checked;
+      if (journaling) {
+        std::lock_guard<std::mutex> lk(journal_mu);
+        std::string jerr;
+        gbj::Record rec{pending[b].first, pending[b].second, r.checked, r.phase2_fallbacks,
+                        r.failures, r.failures ? r.first_failure_n : 0, r.max_minp};
+        if (!journal.append(rec, &jerr)) {
+          W.st = GB_EINVAL;
+          W.err = jerr;
+          stop = true;
+          return;
+        }
+        if (stop_after && ++recorded >= stop_after && !stop.load()) {
+          interrupted = true;
+          stop = true;
+        }
+      }
       if (single_call) break;
     }
   };
@@ -279,7 +354,7 @@ int main(int argc, char** argv) {
     if (progress_thread.joinable()) progress_thread.join();
   }
 
-  Worker sum;
+  Worker sum = prior;
   bool sys_err = false;
   for (int g = 0; g < use_gpus; ++g) {
     if (w[g].st != GB_OK) {
@@ -299,6 +374,11 @@ int main(int argc, char** argv) {
   if (sys_err) {
     std::cerr << "\n[!] Program aborted due to internal hardware/CUDA errors.\n";
     return 1;
+  }
+  if (interrupted.load() && !sum.failures && processed.load() < total) {
+    std::cout << "\nStopped after " << recorded.load() << " journal records ("
+              << processed.load() << " of " << total << " numbers); rerun the same command to resume.\n";
+    return 3;
   }
   if (json) {
     std::printf("{\"start\": %" PRIu64 ", \"limit\": %" PRIu64 ", \"checked\": %" PRIu64

@@ -65,3 +65,32 @@ def test_single_check_1e12():  # validation.sh Test 1.2
     m = re.search(r"1000000000000 = (\d+) \+ (\d+)", out)
     assert m and int(m.group(1)) + int(m.group(2)) == 10**12
     assert int(m.group(1)) <= 194267
+
+
+def test_journal_interrupt_and_resume(tmp_path):
+    """A run stopped after 3 journal records, a torn write appended, then
+    the same command resumes: same summary as one uninterrupted run, every
+    segment journaled exactly once."""
+    j = tmp_path / "j.txt"
+    args = (2000000000, "--seg-size=67108864", "--p-small=1000000")  # 15 segments
+    rc, out = run("goldbach", *args, f"--journal={j}", "--journal-segments=2",
+                  "--stop-after-batches=3")
+    assert rc == 3 and "rerun the same command to resume" in out, out
+    assert len(j.read_text().splitlines()) == 4
+    with open(j, "a") as f:
+        f.write("seg 6 8 checked 1342")  # the write an interruption tore
+    rc, out2 = run("goldbach", *args, f"--journal={j}", "--journal-segments=2")
+    assert rc == 0 and "6 of 15 segments done, 5 batches to run" in out2, out2
+    rc, ref = run("goldbach", *args)
+    assert rc == 0
+    for key in ("satisfy Goldbach. ✓", "Phase 2 fallbacks      :", "Max minimal p          :"):
+        a = [l for l in out2.splitlines() if key in l]
+        b = [l for l in ref.splitlines() if key in l]
+        assert a == b and a, (key, a, b)
+    segs = []
+    checked = 0
+    for line in j.read_text().splitlines()[1:]:
+        f = line.split()
+        segs += list(range(int(f[1]), int(f[2])))
+        checked += int(f[4])
+    assert sorted(segs) == list(range(15)) and checked == 999999999
