@@ -264,6 +264,26 @@ def measure_single(gb, ctx, count=10**6):
             "checksum_p": int(p.astype(np.uint64).sum())}
 
 
+def measure_counts(gb, ctx, points=((10**9, 4096), (10**10, 1024))):
+    """Partition counts c(n) (gb_goldbach_counts) for `count` consecutive even
+    n from n0; one call each (its odd-prime bitset sieve included), the mean
+    of three after a warm-up."""
+    out = []
+    for n0, count in points:
+        ctx.goldbach_counts(n0, 32)
+        walls = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            c = ctx.goldbach_counts(n0, count)
+            walls.append(time.perf_counter() - t0)
+        w = statistics.mean(walls)
+        # scalar (n, p) tests the reference's goldbach_count makes: n/2 - 1 per n
+        tests = sum((n0 + 2 * j) // 2 - 1 for j in range(count))
+        out.append({"n0": n0, "count": count, "ms": w * 1e3, "value": count / w, "unit": "n/s",
+                    "pair_tests_per_s": tests / w, "c_first": int(c[0])})
+    return out
+
+
 def measure_serving(gb, device, rates=(1e2, 1e3, 1e4, 1e5), seconds=2.0, max_requests=10000):
     """C5: Poisson arrivals (seed 3) per rate; 70% single n uniform in
     [4, 2^64-2], 30% ranges of log-uniform width 2^8..2^26 even n at
@@ -489,6 +509,7 @@ def main():
             with gb.Context(local) as c2:
                 out["windows"] = measure_windows(gb, c2)
                 out["single"] = measure_single(gb, c2)
+                out["counts"] = measure_counts(gb, c2)
             out["serving"] = measure_serving(gb, local)
     if rank == 0:
         print(json.dumps(out))

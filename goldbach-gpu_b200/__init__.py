@@ -61,6 +61,10 @@ class RangeOut(C.Structure):
                 ("seg_fallbacks", vp), ("seg_failures", vp), ("seg_hist", vp)]
 
 
+class CountOpts(C.Structure):
+    _fields_ = [("on_device", C.c_int), ("stream", C.c_void_p)]
+
+
 class SingleOpts(C.Structure):
     _fields_ = [("p_limit", u64), ("on_device", i32), ("stream", vp)]
 
@@ -142,6 +146,7 @@ def load(path: str = LIB_PATH):
         "gb_num_segments": (u64, [u64, u64, u64]),
         "gb_verify_range": (i32, [vp, u64, u64, P(RangeOpts), P(RangeResult), P(RangeOut)]),
         "gb_sieve_bitset": (i32, [vp, u64, u64, vp, i32, vp]),
+        "gb_goldbach_counts": (i32, [vp, u64, u64, vp, P(CountOpts)]),
         "gb_primes_upto": (i32, [vp, u64, vp, u64, P(u64)]),
         "gb_is_prime_batch": (i32, [vp, vp, C.c_size_t, vp, i32, vp]),
         "gb_check_single_batch": (i32, [vp, vp, C.c_size_t, vp, vp, P(SingleOpts), P(SingleResult)]),
@@ -277,6 +282,18 @@ class Context:
         w = np.zeros((nbits + 31) // 32, np.uint32)
         self._check(self.L.gb_sieve_bitset(self._h, q_lo, nbits, w.ctypes.data, 0, None))
         return w
+
+    def goldbach_counts(self, start: int, count: int, device_out=None, stream=None) -> np.ndarray:
+        """c(n) = #{p <= n/2 : p, n - p prime} for n = start, start + 2, ...
+        (count values; gb_goldbach_counts).  device_out: a device buffer
+        (torch int64 tensor) to fill instead of returning a host array."""
+        o = CountOpts(1 if device_out is not None else 0, stream)
+        if device_out is not None:
+            self._check(self.L.gb_goldbach_counts(self._h, start, count, _ptr(device_out), C.byref(o)))
+            return device_out
+        out = np.zeros(count, np.uint64)
+        self._check(self.L.gb_goldbach_counts(self._h, start, count, out.ctypes.data, C.byref(o)))
+        return out
 
     def primes_upto(self, limit: int) -> np.ndarray:
         n = u64()

@@ -12,7 +12,9 @@
 // VRAM guard), --json (one JSON summary line at the end), --journal=FILE
 // (resumable runs, journal.h) with --journal-segments=K (segments per
 // record) and --stop-after-batches=N (end the run after N new records, exit
-// code 3: the way tests interrupt a run).
+// code 3: the way tests interrupt a run), --counts (print c(n), the number
+// of Goldbach partitions, for every even n of [START, LIMIT] in the
+// reference's `c(n) = k` form, src/cpu_goldbach.cpp:100-103).
 #include <atomic>
 #include <chrono>
 #include <cinttypes>
@@ -55,6 +57,7 @@ void print_usage(const char* prog) {
             << "  --journal=FILE   Record completed segments in FILE; rerun to resume\n"
             << "  --journal-segments=K  Segments per journal record (default: about 2^36 n)\n"
             << "  --stop-after-batches=N  Stop after N new journal records (exit code 3)\n"
+            << "  --counts         Print c(n) = number of partitions for each even n\n"
             << "  -h, --help       Show this help message\n";
 }
 
@@ -73,7 +76,7 @@ int main(int argc, char** argv) {
     print_usage(argv[0]);
     return 0;
   }
-  bool show_progress = false, json = false;
+  bool show_progress = false, json = false, counts_mode = false;
   uint64_t LIMIT = 0, SEG_SIZE = 10'000'000ULL, P_SMALL = 1'000'000ULL, START = 4;
   uint64_t chunk = 0, halo = 0, phase2 = 0, mem_mb = 0, batch = 100000;
   std::string journal_path;
@@ -90,6 +93,7 @@ int main(int argc, char** argv) {
       if (arg == "--async") continue;
       if (arg == "--progress") { show_progress = true; continue; }
       if (arg == "--json") { json = true; continue; }
+      if (arg == "--counts") { counts_mode = true; continue; }
       if (arg.rfind("--batch-size=", 0) == 0) { batch = std::stoull(arg.substr(13)); continue; }
       if (arg.rfind("--gpus=", 0) == 0) { requested_gpus = std::stol(arg.substr(7)); continue; }
       if (arg.rfind("--seg-size=", 0) == 0) { SEG_SIZE = std::stoull(arg.substr(11)); continue; }
@@ -145,6 +149,42 @@ int main(int argc, char** argv) {
   const uint64_t p2 = phase2 ? phase2 : GB_PHASE2_LIMIT_DEFAULT;
   const uint64_t total = (LIMIT - START) / 2 + 1;
   const uint64_t nseg = (total + SEG_SIZE - 1) / SEG_SIZE;
+
+  // Partition counts: c(n) for every even n of [START, LIMIT], on GPU 0.
+  if (counts_mode) {
+    if (gb_device_count() == 0) {
+      std::cerr << "No CUDA devices found.\n";
+      return 1;
+    }
+    gb_config ccfg{};
+    ccfg.device_mem_budget = mem_mb << 20;
+    gb_ctx* cctx = nullptr;
+    gb_status st = gb_create(0, &ccfg, &cctx);
+    if (st != GB_OK) {
+      std::cerr << "[!] FATAL ERROR in GPU 0 Worker: " << gb_strerror(st) << "\n";
+      return 1;
+    }
+    const uint64_t per = 1ull << 16;
+    std::vector<uint64_t> c(per);
+    auto tc = clk::now();
+    for (uint64_t j = 0; j < total && st == GB_OK; j += per) {
+      const uint64_t k = std::min(per, total - j);
+      st = gb_goldbach_counts(cctx, START + 2 * j, k, c.data(), nullptr);
+      for (uint64_t i = 0; st == GB_OK && i < k; ++i)
+        std::printf("c(%" PRIu64 ") = %" PRIu64 "\n", START + 2 * (j + i), c[i]);
+    }
+    if (st != GB_OK) {
+      std::cerr << "[!] FATAL ERROR in GPU 0 Worker: " << gb_strerror(st) << " (" << gb_last_error(cctx) << ")\n";
+      gb_destroy(cctx);
+      return 1;
+    }
+    gb_destroy(cctx);
+    std::fflush(stdout);
+    std::cout << "\n--- Summary ---\n";
+    std::cout << "Even numbers counted : " << total << "\n";
+    std::cout << "Total time           : " << std::chrono::duration<double, std::milli>(clk::now() - tc).count() << " ms\n";
+    return 0;
+  }
 
   // The journal: what earlier runs of this command finished.
   gbj::Journal journal;

@@ -119,6 +119,8 @@ struct WindowsArgs {
 // kernels/tables.cu
 cudaError_t launch_wheel_init(uint32_t* wheel, uint32_t* wheel6, cudaStream_t s);
 cudaError_t launch_sieve_bits(const SieveArgs& a, cudaStream_t s);
+cudaError_t launch_counts(const uint32_t* B, uint64_t m_first, uint64_t count, uint32_t splits,
+                          uint64_t wps, unsigned long long* out, cudaStream_t s);
 // Appends the primes of `bits` (odd-only from q_lo) after `prefix` entries of
 // `primes`; writes the new total into *d_total (device) and magic[] for them.
 cudaError_t launch_compact_primes(const uint32_t* bits, uint64_t nbits, uint64_t q_lo,

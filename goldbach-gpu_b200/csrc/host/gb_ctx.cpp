@@ -729,6 +729,72 @@ gb_status gb_sieve_bitset(gb_ctx* c, uint64_t q_lo, uint64_t nbits, uint32_t* wo
   GB_PUBLIC(c, sieve_bitset_impl(c, c->ws, q_lo, nbits, words, on_device, stream));
 }
 
+// Partition counts (kernels/counts.cu): the odd-prime bitset of [1, n_max]
+// is sieved into a padded device buffer (two zero words in front, slack
+// behind for the correlation's 64-bit windows), then one warp per 32
+// consecutive n and slice of the bitset's words.
+static gb_status counts_impl(gb_ctx* c, Workspace& w, uint64_t start, uint64_t count,
+                             uint64_t* counts, const gb_count_opts* opts) {
+  if (!count) return GB_OK;
+  if (!counts) return fail(w, GB_EINVAL, "null counts");
+  if (start < 4) start = 4;
+  if (start & 1) start++;
+  if (count > (GB_COUNTS_MAX_N - start) / 2 + 1 || start > GB_COUNTS_MAX_N)
+    return fail(w, GB_EINVAL, "n above the partition-count limit (2^40)");
+  gb_count_opts o{};
+  if (opts) o = *opts;
+  const uint64_t n_max = start + 2 * (count - 1);
+  const uint64_t nbits = (n_max - 1) / 2 + 1;  // odd q = 1 .. n_max - 1
+  const uint64_t nwords = (nbits + 31) / 32;
+  gb_status st = ensure_primes(c, w, isqrt_u64(n_max) + 2);
+  if (st != GB_OK) return st;
+  cudaStream_t s = o.stream ? (cudaStream_t)o.stream : c->stream;
+  Temps tmp(c, nullptr);
+  uint32_t* buf = nullptr;
+  unsigned long long* d_out = (unsigned long long*)counts;
+  if ((st = tmp.get((nwords + 8) * 4, (void**)&buf, w)) != GB_OK) return st;
+  if (!o.on_device && (st = tmp.get(count * 8, (void**)&d_out, w)) != GB_OK) return st;
+  const uint32_t tile = 1u << 18;
+  const uint64_t root = isqrt_u64(n_max);
+  uint64_t ns = 0, kc = 0;
+  if ((st = count_le(c, w, root, &ns)) != GB_OK || (st = count_le(c, w, tile / 64, &kc)) != GB_OK)
+    return st;
+  SieveArgs a{};
+  a.q_lo = 1;
+  a.nbits = nbits;
+  a.tile_bits = tile;
+  a.primes = c->d_primes;
+  a.magic = c->d_magic;
+  a.nsieve = (uint32_t)std::max<uint64_t>(ns, kWheelPrimeCount + 1);
+  a.kcoop = (uint32_t)std::max<uint64_t>(std::min(kc, ns), kWheelPrimeCount + 1);
+  a.wheel = c->d_wheel;
+  a.out = buf + 2;
+  // Work split: enough warp tasks to fill the GPU, at most 2^22 words each.
+  const uint64_t groups = (count + 31) / 32;
+  const uint64_t wmax = n_max / 4 / 32 + 1;  // words of i for the largest n
+  uint64_t splits = std::max<uint64_t>(1, ((uint64_t)c->sm_count * 64 + groups - 1) / groups);
+  splits = std::max<uint64_t>(splits, (wmax + (1u << 22) - 1) >> 22);
+  uint64_t wps = (wmax + splits - 1) / splits;
+  wps = std::max<uint64_t>(32, (wps + 31) & ~31ull);
+  splits = (wmax + wps - 1) / wps;
+  cudaError_t e = cudaMemsetAsync(buf, 0, (nwords + 8) * 4, s);
+  if (e == cudaSuccess) e = launch_sieve_bits(a, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_out, 0, count * 8, s);
+  if (e == cudaSuccess) e = cudaEventRecord(w.ek0, s);
+  if (e == cudaSuccess) e = launch_counts(buf + 2, start / 2 - 1, count, (uint32_t)splits, wps, d_out, s);
+  if (e == cudaSuccess) e = cudaEventRecord(w.ek1, s);
+  if (e == cudaSuccess && !o.on_device) e = cudaMemcpyAsync(counts, d_out, count * 8, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(w, e, "partition counts");
+  return GB_OK;
+}
+
+gb_status gb_goldbach_counts(gb_ctx* c, uint64_t start, uint64_t count, uint64_t* counts,
+                             const gb_count_opts* opts) {
+  if (!c) return GB_EINVAL;
+  GB_PUBLIC(c, counts_impl(c, c->ws, start, count, counts, opts));
+}
+
 static gb_status primes_upto_impl(gb_ctx* c, Workspace& w, uint64_t limit, uint32_t* primes,
                                   uint64_t cap, uint64_t* count) {
   if (!count) return fail(w, GB_EINVAL, "null count");

@@ -142,6 +142,23 @@ gb_status gb_verify_range(gb_ctx* ctx, uint64_t start, uint64_t limit,
                           const gb_range_out* out);
 
 /* -------------------------------------------------------------------------
+ * Goldbach partition counts: counts[j] = c(n) for n = start + 2j, j < count,
+ * where c(n) = #{p <= n/2 : p and n - p prime} (so c(4) = 1, c(6) = 1,
+ * c(10) = 2).  Replaces goldbach_count (src/cpu_goldbach.cpp:29-36), the
+ * reference's CPU-only scan behind its c(n) roadmap item (RESULTS.md:169).
+ * start < 4 -> 4, odd start -> start + 1; n up to GB_COUNTS_MAX_N.  The
+ * call holds the odd-prime bitset of [1, n_max] on the device (n_max / 16
+ * bytes).  counts is host memory, or device memory with opts->on_device.
+ * ---------------------------------------------------------------------- */
+#define GB_COUNTS_MAX_N (1ull << 40)
+typedef struct {
+  int on_device;  /* counts is a device pointer */
+  void* stream;   /* cudaStream_t; NULL: the context's stream */
+} gb_count_opts;
+gb_status gb_goldbach_counts(gb_ctx* ctx, uint64_t start, uint64_t count, uint64_t* counts,
+                             const gb_count_opts* opts);
+
+/* -------------------------------------------------------------------------
  * Odd-only prime bitset of a window (the GPU sieve on its own): bit i of
  * `words` <-> odd q_lo + 2*i is prime.  Replaces build_prime_bitset
  * (src/prime_bitset.cpp:21-97) and the tiled sieve's output layout

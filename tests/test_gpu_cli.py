@@ -94,3 +94,14 @@ def test_journal_interrupt_and_resume(tmp_path):
         segs += list(range(int(f[1]), int(f[2])))
         checked += int(f[4])
     assert sorted(segs) == list(range(15)) and checked == 999999999
+
+
+def test_counts_mode(tmp_path):
+    """goldbach --counts prints the reference's `c(n) = k` lines."""
+    import json
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "ref_goldbach_count.json")))
+    rc, out = run("goldbach", 2000, "--counts")
+    assert rc == 0, out
+    lines = [l for l in out.splitlines() if l.startswith("c(")]
+    want = [f"c({g['first_n'] + 2 * j}) = {v}" for j, v in enumerate(g["counts"]) if g["first_n"] + 2 * j <= 2000]
+    assert lines == want and "Even numbers counted : 999" in out
