@@ -129,32 +129,52 @@ __device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ 
   //    (stride 32p stays far below 2^32: these primes are < nbits / 64).
   const uint32_t kfirst = kWheelPrimeCount + 1;
   const uint32_t kc = kcoop < nsieve ? kcoop : nsieve;
-  for (uint32_t k = kfirst + warp; k < kc; k += NW) {
-    const uint32_t p = __ldg(primes + k);
-    if ((uint64_t)p * p > q_top) break;
-    uint32_t t1, t5;
-    first_marks6(G0, p, __ldg(a15 + k), base_mod(G0, p, __ldg(magic + k)), nbits, t1, t5);
-    const uint32_t stride = 32 * p;
-    for (uint32_t i = t1 + lane * p; i < nbits; i += stride)
-      atomicAnd(&Q1[i >> 5], ~(1u << (i & 31)));
-    for (uint32_t i = t5 + lane * p; i < nbits; i += stride)
-      atomicAnd(&Q5[i >> 5], ~(1u << (i & 31)));
+  {  // the next prime's table entries are loaded one iteration ahead
+    uint32_t k = kfirst + warp;
+    uint32_t pn = 0;
+    uint64_t mn = 0;
+    uint2 an = make_uint2(0, 0);
+    if (k < kc) { pn = __ldg(primes + k); mn = __ldg(magic + k); an = __ldg(a15 + k); }
+    for (; k < kc; k += NW) {
+      const uint32_t p = pn;
+      const uint64_t mg = mn;
+      const uint2 ac = an;
+      if (k + NW < kc) { pn = __ldg(primes + k + NW); mn = __ldg(magic + k + NW); an = __ldg(a15 + k + NW); }
+      if ((uint64_t)p * p > q_top) break;
+      uint32_t t1, t5;
+      first_marks6(G0, p, ac, base_mod(G0, p, mg), nbits, t1, t5);
+      const uint32_t stride = 32 * p;
+      for (uint32_t i = t1 + lane * p; i < nbits; i += stride)
+        atomicAnd(&Q1[i >> 5], ~(1u << (i & 31)));
+      for (uint32_t i = t5 + lane * p; i < nbits; i += stride)
+        atomicAnd(&Q5[i >> 5], ~(1u << (i & 31)));
+    }
   }
   // 4. one thread per prime for the rest, both classes in one loop; the
   //    steps are taken only while they stay below nbits (p may be near 2^32).
-  for (uint32_t k = (kc > kfirst ? kc : kfirst) + tid; k < nsieve; k += NT) {
-    const uint32_t p = __ldg(primes + k);
-    if ((uint64_t)p * p > q_top) break;
-    uint32_t j1, j5;
-    first_marks6(G0, p, __ldg(a15 + k), base_mod(G0, p, __ldg(magic + k)), nbits, j1, j5);
-    while (j1 < nbits || j5 < nbits) {
-      if (j1 < nbits) {
-        atomicAnd(&Q1[j1 >> 5], ~(1u << (j1 & 31)));
-        j1 = nbits - j1 > p ? j1 + p : nbits;
-      }
-      if (j5 < nbits) {
-        atomicAnd(&Q5[j5 >> 5], ~(1u << (j5 & 31)));
-        j5 = nbits - j5 > p ? j5 + p : nbits;
+  {  // the next prime's table entries are loaded one iteration ahead
+    uint32_t k = (kc > kfirst ? kc : kfirst) + tid;
+    uint32_t pn = 0;
+    uint64_t mn = 0;
+    uint2 an = make_uint2(0, 0);
+    if (k < nsieve) { pn = __ldg(primes + k); mn = __ldg(magic + k); an = __ldg(a15 + k); }
+    for (; k < nsieve; k += NT) {
+      const uint32_t p = pn;
+      const uint64_t mg = mn;
+      const uint2 ac = an;
+      if (k + NT < nsieve) { pn = __ldg(primes + k + NT); mn = __ldg(magic + k + NT); an = __ldg(a15 + k + NT); }
+      if ((uint64_t)p * p > q_top) break;
+      uint32_t j1, j5;
+      first_marks6(G0, p, ac, base_mod(G0, p, mg), nbits, j1, j5);
+      while (j1 < nbits || j5 < nbits) {
+        if (j1 < nbits) {
+          atomicAnd(&Q1[j1 >> 5], ~(1u << (j1 & 31)));
+          j1 = nbits - j1 > p ? j1 + p : nbits;
+        }
+        if (j5 < nbits) {
+          atomicAnd(&Q5[j5 >> 5], ~(1u << (j5 & 31)));
+          j5 = nbits - j5 > p ? j5 + p : nbits;
+        }
       }
     }
   }
