@@ -87,6 +87,10 @@ __global__ void __launch_bounds__(kRangeThreads, 2) range_kernel(const __grid_co
 // q-window is the two class bitsets Q1 / Q5 (no multiple of 3 stored), and
 // the n of a chunk are searched by class n mod 6.
 
+// threads per CTA and CTAs per SM of range6_kernel
+constexpr int kRange6Threads = 512;
+constexpr int kRange6Blocks = 2;
+
 // floor((A - H - 1) / 6) for A possibly below H
 __device__ __forceinline__ int64_t window_g0(uint64_t A, uint32_t H) {
   if (A >= (uint64_t)H + 1) return (int64_t)((A - H - 1) / 6);
@@ -94,13 +98,13 @@ __device__ __forceinline__ int64_t window_g0(uint64_t A, uint32_t H) {
 }
 
 template <bool MINP>
-__global__ void __launch_bounds__(kRangeThreads, 2) range6_kernel(const __grid_constant__ RangeArgs a) {
+__global__ void __launch_bounds__(kRange6Threads, kRange6Blocks) range6_kernel(const __grid_constant__ RangeArgs a) {
   const SearchParams& s = a.s;
   __shared__ unsigned long long s_item;
   const int tid = threadIdx.x;
   Ctx6& cx = g_cx6;
   uint32_t* pat6 = smem6_pat();
-  for (uint32_t i = tid; i < kWheel6Words; i += kRangeThreads) pat6[i] = a.wheel6[i];
+  for (uint32_t i = tid; i < kWheel6Words; i += kRange6Threads) pat6[i] = a.wheel6[i];
   if (tid == 0) cx.nbw = a.nbw;
   __syncthreads();
   load_tables6(s);
@@ -120,7 +124,7 @@ __global__ void __launch_bounds__(kRangeThreads, 2) range6_kernel(const __grid_c
       cx.scnt[0] = cx.scnt[1] = cx.scnt[2] = 0;
       cx.maxk = 0;
     }
-    for (uint32_t i = tid; i < kSmemHistBins; i += kRangeThreads) HIST[i] = 0;
+    for (uint32_t i = tid; i < kSmemHistBins; i += kRange6Threads) HIST[i] = 0;
     __syncthreads();
     const unsigned long long item = s_item;
     if (item >= a.total_items) break;
@@ -157,9 +161,9 @@ __global__ void __launch_bounds__(kRangeThreads, 2) range6_kernel(const __grid_c
       }
     }
     const uint32_t nbits = s.halo / 6 + cnt / 3 + 96;
-    sieve_window6<kRangeThreads>(Q1, Q5, a.nbw, nbits, G0, A + 2ull * cnt, pat6, s.primes,
+    sieve_window6<kRange6Threads>(Q1, Q5, a.nbw, nbits, G0, A + 2ull * cnt, pat6, s.primes,
                                  a.magic, a.a15, a.nsieve, a.kcoop);
-    search_chunk6<MINP, kRangeThreads>(s, surv, a.surv_cap);
+    search_chunk6<MINP, kRange6Threads>(s, surv, a.surv_cap);
   }
 }
 
@@ -242,32 +246,35 @@ size_t range_smem_bytes(const RangeArgs& a) {
 }
 
 template <typename K>
-static int occupancy(K kernel, size_t smem) {
+static int occupancy(K kernel, size_t smem, int threads = kRangeThreads) {
   int nb = 0;
   cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, kRangeThreads, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, smem);
   return nb;
 }
 
 int range_max_blocks_per_sm(const RangeArgs& a) {
   const size_t smem = range_smem_bytes(a);
-  if (a.layout6) return a.s.minp ? occupancy(range6_kernel<true>, smem) : occupancy(range6_kernel<false>, smem);
+  if (a.layout6)
+    return a.s.minp ? occupancy(range6_kernel<true>, smem, kRange6Threads)
+                    : occupancy(range6_kernel<false>, smem, kRange6Threads);
   return a.s.minp ? occupancy(range_kernel<true>, smem) : occupancy(range_kernel<false>, smem);
 }
 
 template <typename K>
-static cudaError_t launch_one(K kernel, const RangeArgs& a, int grid, size_t smem, cudaStream_t st) {
+static cudaError_t launch_one(K kernel, const RangeArgs& a, int grid, size_t smem, cudaStream_t st,
+                              int threads = kRangeThreads) {
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  kernel<<<grid, kRangeThreads, smem, st>>>(a);
+  kernel<<<grid, threads, smem, st>>>(a);
   return cudaGetLastError();
 }
 
 cudaError_t launch_range(const RangeArgs& a, int grid, cudaStream_t st) {
   const size_t smem = range_smem_bytes(a);
   if (a.layout6)
-    return a.s.minp ? launch_one(range6_kernel<true>, a, grid, smem, st)
-                    : launch_one(range6_kernel<false>, a, grid, smem, st);
+    return a.s.minp ? launch_one(range6_kernel<true>, a, grid, smem, st, kRange6Threads)
+                    : launch_one(range6_kernel<false>, a, grid, smem, st, kRange6Threads);
   return a.s.minp ? launch_one(range_kernel<true>, a, grid, smem, st)
                   : launch_one(range_kernel<false>, a, grid, smem, st);
 }

@@ -166,6 +166,11 @@ __device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ 
       if ((uint64_t)p * p > q_top) break;
       uint32_t j1, j5;
       first_marks6(G0, p, ac, base_mod(G0, p, mg), nbits, j1, j5);
+      if (p >= nbits) {  // at most one multiple per class: no loop (no divergent exits)
+        if (j1 < nbits) atomicAnd(&Q1[j1 >> 5], ~(1u << (j1 & 31)));
+        if (j5 < nbits) atomicAnd(&Q5[j5 >> 5], ~(1u << (j5 & 31)));
+        continue;
+      }
       while (j1 < nbits || j5 < nbits) {
         if (j1 < nbits) {
           atomicAnd(&Q1[j1 >> 5], ~(1u << (j1 & 31)));
