@@ -46,6 +46,14 @@ class RangeOpts(C.Structure):
                 ("shard_count", u32), ("on_device", i32), ("stream", vp)]
 
 
+class AutotuneResult(C.Structure):
+    _fields_ = [("chunk_evens", u32), ("halo", u32), ("even_n_per_s", C.c_double),
+                ("candidates", u32), ("sample_evens", u64), ("cached", i32)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class RangeResult(C.Structure):
     _fields_ = [("checked", u64), ("verified", u64), ("phase2_fallbacks", u64),
                 ("failures", u64), ("first_failure_n", u64), ("max_minp", u64),
@@ -147,6 +155,7 @@ def load(path: str = LIB_PATH):
         "gb_verify_range": (i32, [vp, u64, u64, P(RangeOpts), P(RangeResult), P(RangeOut)]),
         "gb_sieve_bitset": (i32, [vp, u64, u64, vp, i32, vp]),
         "gb_goldbach_counts": (i32, [vp, u64, u64, vp, P(CountOpts)]),
+        "gb_autotune_range": (i32, [vp, u64, u64, P(RangeOpts), P(RangeOpts), P(AutotuneResult)]),
         "gb_primes_upto": (i32, [vp, u64, vp, u64, P(u64)]),
         "gb_is_prime_batch": (i32, [vp, vp, C.c_size_t, vp, i32, vp]),
         "gb_check_single_batch": (i32, [vp, vp, C.c_size_t, vp, vp, P(SingleOpts), P(SingleResult)]),
@@ -229,6 +238,17 @@ class Context:
         return held.value, budget.value
 
     # -- range -------------------------------------------------------------
+    def autotune_range(self, start: int, limit: int, *, seg_size: int = 10_000_000,
+                       p_small: int = 1_000_000, phase2_limit: int = 0) -> dict:
+        """gb_autotune_range: the chunk_evens and halo to use for [start, limit]
+        (timed on a sample at the top of the range, cached per range class)."""
+        base = RangeOpts(seg_size, p_small, phase2_limit, 0, 0, 0, 1, 0, None)
+        tuned = RangeOpts()
+        r = AutotuneResult()
+        self._check(self.L.gb_autotune_range(self._h, start, limit, C.byref(base), C.byref(tuned),
+                                             C.byref(r)))
+        return r.as_dict()
+
     def verify_range(self, start: int, limit: int, *, seg_size: int = 10_000_000,
                      p_small: int = 1_000_000, phase2_limit: int = 0, chunk: int = 0,
                      halo: int = 0, shard_index: int = 0, shard_count: int = 1,

@@ -14,12 +14,18 @@
 // record) and --stop-after-batches=N (end the run after N new records, exit
 // code 3: the way tests interrupt a run), --counts (print c(n), the number
 // of Goldbach partitions, for every even n of [START, LIMIT] in the
-// reference's `c(n) = k` form, src/cpu_goldbach.cpp:100-103).
+// reference's `c(n) = k` form, src/cpu_goldbach.cpp:100-103), --autotune
+// (pick chunk and halo with gb_autotune_range; --autotune-cache=FILE keeps
+// the choice per range class across runs), --tile=N (the same as --chunk),
+// --minp-out=FILE (the minimal p of every n, uint32 little-endian, in range
+// order) and --bitmap-out=FILE (the verified bit of every n, bit j of byte
+// j/8 for n = START + 2j); the output files are written from GPU 0 in order.
 #include <atomic>
 #include <chrono>
 #include <cinttypes>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
 #include <iomanip>
 #include <iostream>
 #include <mutex>
@@ -58,8 +64,43 @@ void print_usage(const char* prog) {
             << "  --journal-segments=K  Segments per journal record (default: about 2^36 n)\n"
             << "  --stop-after-batches=N  Stop after N new journal records (exit code 3)\n"
             << "  --counts         Print c(n) = number of partitions for each even n\n"
+            << "  --autotune       Pick chunk and halo for this range by timing a sample\n"
+            << "  --autotune-cache=FILE  Reuse / record autotuned choices per range class\n"
+            << "  --tile=N         Same as --chunk=N\n"
+            << "  --minp-out=FILE  Write the minimal p of every n (uint32, in order)\n"
+            << "  --bitmap-out=FILE Write the verified bit of every n (bit j <-> START+2j)\n"
             << "  -h, --help       Show this help message\n";
 }
+
+// Appends bit strings to a file whatever their alignment: bit j of the
+// stream is bit j % 8 of byte j / 8.
+struct BitWriter {
+  FILE* f;
+  uint32_t carry = 0;  // pending low bits of the next byte
+  int ncarry = 0;
+  bool put(const uint32_t* words, uint64_t nbits) {
+    std::vector<uint8_t> out;
+    out.reserve(nbits / 8 + 2);
+    for (uint64_t i = 0; i < nbits; i += 8) {
+      const uint64_t take = nbits - i < 8 ? nbits - i : 8;
+      uint32_t b = (words[i >> 5] >> (i & 31)) & ((1u << take) - 1);
+      carry |= b << ncarry;
+      ncarry += (int)take;
+      if (ncarry >= 8) {
+        out.push_back((uint8_t)(carry & 0xff));
+        carry >>= 8;
+        ncarry -= 8;
+      }
+    }
+    return std::fwrite(out.data(), 1, out.size(), f) == out.size();
+  }
+  bool finish() {
+    if (!ncarry) return true;
+    const uint8_t b = (uint8_t)carry;
+    ncarry = 0;
+    return std::fwrite(&b, 1, 1, f) == 1;
+  }
+};
 
 struct Worker {
   gb_ctx* ctx = nullptr;
@@ -79,7 +120,8 @@ int main(int argc, char** argv) {
   bool show_progress = false, json = false, counts_mode = false;
   uint64_t LIMIT = 0, SEG_SIZE = 10'000'000ULL, P_SMALL = 1'000'000ULL, START = 4;
   uint64_t chunk = 0, halo = 0, phase2 = 0, mem_mb = 0, batch = 100000;
-  std::string journal_path;
+  std::string journal_path, tune_cache, minp_path, bitmap_path;
+  bool autotune = false;
   uint64_t journal_segs = 0, stop_after = 0;
   long requested_gpus = 1;
   std::vector<std::string> positional;
@@ -94,6 +136,11 @@ int main(int argc, char** argv) {
       if (arg == "--progress") { show_progress = true; continue; }
       if (arg == "--json") { json = true; continue; }
       if (arg == "--counts") { counts_mode = true; continue; }
+      if (arg == "--autotune") { autotune = true; continue; }
+      if (arg.rfind("--autotune-cache=", 0) == 0) { tune_cache = arg.substr(17); autotune = true; continue; }
+      if (arg.rfind("--tile=", 0) == 0) { chunk = std::stoull(arg.substr(7)); continue; }
+      if (arg.rfind("--minp-out=", 0) == 0) { minp_path = arg.substr(11); continue; }
+      if (arg.rfind("--bitmap-out=", 0) == 0) { bitmap_path = arg.substr(13); continue; }
       if (arg.rfind("--batch-size=", 0) == 0) { batch = std::stoull(arg.substr(13)); continue; }
       if (arg.rfind("--gpus=", 0) == 0) { requested_gpus = std::stol(arg.substr(7)); continue; }
       if (arg.rfind("--seg-size=", 0) == 0) { SEG_SIZE = std::stoull(arg.substr(11)); continue; }
@@ -186,6 +233,12 @@ int main(int argc, char** argv) {
     return 0;
   }
 
+  const bool outputs = !minp_path.empty() || !bitmap_path.empty();
+  if (outputs && !journal_path.empty()) {
+    std::cerr << "Error: --minp-out / --bitmap-out cannot be combined with --journal.\n";
+    return 1;
+  }
+
   // The journal: what earlier runs of this command finished.
   gbj::Journal journal;
   Worker prior;  // journaled figures
@@ -234,7 +287,11 @@ int main(int argc, char** argv) {
     std::cerr << "Requested " << requested_gpus << " GPUs, but only " << device_count
               << " available. Using " << device_count << ".\n";
   }
-  const int use_gpus = (requested_gpus <= 0 || requested_gpus > device_count) ? device_count : (int)requested_gpus;
+  int use_gpus = (requested_gpus <= 0 || requested_gpus > device_count) ? device_count : (int)requested_gpus;
+  if (outputs && use_gpus > 1) {
+    std::cout << "Per-n outputs are written in order from GPU 0: using 1 GPU.\n";
+    use_gpus = 1;
+  }
 
   // VRAM guard (src/goldbach.cu:505-541) against what a context will hold;
   // --device-mem-mb caps the available memory.
@@ -271,6 +328,53 @@ int main(int argc, char** argv) {
     }
   }
   std::cout << "Pre-generating device primes up to " << std::max(P_SMALL, p2) << "...\n";
+  if (autotune) {
+    // one line per range class: "class BITS P_SMALL PHASE2 chunk C halo H"
+    uint64_t bits = 0;
+    for (uint64_t x = LIMIT; x; x >>= 1) ++bits;
+    char key[128];
+    std::snprintf(key, sizeof key, "class %" PRIu64 " %" PRIu64 " %" PRIu64, bits, P_SMALL, p2);
+    bool found = false;
+    if (!tune_cache.empty()) {
+      std::ifstream in(tune_cache);
+      std::string line;
+      while (std::getline(in, line)) {
+        unsigned long long c = 0, h = 0;
+        const size_t at = line.find(" chunk ");
+        if (at != std::string::npos && line.substr(0, at) == key &&
+            std::sscanf(line.c_str() + at, " chunk %llu halo %llu", &c, &h) == 2) {
+          chunk = c;
+          halo = h;
+          found = true;
+        }
+      }
+      if (found) std::cout << "[Autotune] chunk=" << chunk << " halo=" << halo << " (from " << tune_cache << ")\n";
+    }
+    if (!found) {
+      gb_range_opts base{}, tuned{};
+      base.seg_size = SEG_SIZE;
+      base.p_small = P_SMALL;
+      base.phase2_limit = p2;
+      gb_autotune_result ar{};
+      const gb_status st = gb_autotune_range(w[0].ctx, START, LIMIT, &base, &tuned, &ar);
+      if (st != GB_OK) {
+        std::cerr << "[!] FATAL ERROR in GPU 0 Worker: " << gb_strerror(st) << " (" << gb_last_error(w[0].ctx) << ")\n";
+        return 1;
+      }
+      chunk = tuned.chunk_evens;
+      halo = tuned.halo;
+      if (ar.candidates)
+        std::cout << "[Autotune] chunk=" << chunk << " halo=" << halo << " (" << std::scientific
+                  << std::setprecision(3) << ar.even_n_per_s << " n/s on " << ar.sample_evens
+                  << " n, " << ar.candidates << " candidates)\n" << std::defaultfloat << std::setprecision(6);
+      else
+        std::cout << "[Autotune] range too short to tune: defaults\n";
+      if (!tune_cache.empty() && ar.candidates) {
+        std::ofstream out(tune_cache, std::ios::app);
+        out << key << " chunk " << chunk << " halo " << halo << "\n";
+      }
+    }
+  }
   auto t1 = clk::now();
   std::cout << "Initialization completed in "
             << std::chrono::duration<double, std::milli>(t1 - t0).count() << " ms.\n\n";
@@ -287,6 +391,16 @@ int main(int argc, char** argv) {
   // the GPUs in turn, each recorded when it completes.
   uint64_t segs_per_batch = nseg;
   if (show_progress) segs_per_batch = std::max<uint64_t>(1, (nseg + 63) / 64);
+  if (outputs)  // host buffers of about 2^26 n per call
+    segs_per_batch = std::min(segs_per_batch, std::max<uint64_t>(1, (1ull << 26) / SEG_SIZE));
+  FILE* f_minp = minp_path.empty() ? nullptr : std::fopen(minp_path.c_str(), "wb");
+  FILE* f_bits = bitmap_path.empty() ? nullptr : std::fopen(bitmap_path.c_str(), "wb");
+  if ((!minp_path.empty() && !f_minp) || (!bitmap_path.empty() && !f_bits)) {
+    std::cerr << "Error: cannot open an output file.\n";
+    return 1;
+  }
+  BitWriter bitw{f_bits};
+  std::vector<uint32_t> h_minp, h_bits;
   const uint64_t nbatch = journaling ? pending.size() : (nseg + segs_per_batch - 1) / segs_per_batch;
   std::atomic<uint64_t> processed{prior.checked};
   std::atomic<uint64_t> next_batch{0}, recorded{0};
@@ -296,7 +410,7 @@ int main(int argc, char** argv) {
 
   auto run = [&](int g) {
     Worker& W = w[g];
-    const bool single_call = !show_progress && !journaling;
+    const bool single_call = !show_progress && !journaling && !outputs;
     for (uint64_t b = journaling ? next_batch++ : (uint64_t)g; b < nbatch && !stop.load();
          b = journaling ? next_batch++ : b + use_gpus) {
       gb_range_opts o{};
@@ -318,7 +432,20 @@ int main(int argc, char** argv) {
         e = START + 2 * last_idx;
       }
       gb_range_result r{};
-      gb_status st = gb_verify_range(W.ctx, a, e, &o, &r, nullptr);
+      gb_range_out ro{};
+      const uint64_t bn = (e - a) / 2 + 1;
+      if (f_minp) {
+        h_minp.resize(bn);
+        ro.min_p = h_minp.data();
+      }
+      if (f_bits) {
+        h_bits.resize((bn + 31) / 32);
+        ro.verified_bits = h_bits.data();
+      }
+      gb_status st = gb_verify_range(W.ctx, a, e, &o, &r, outputs ? &ro : nullptr);
+      if (st == GB_OK && f_minp && std::fwrite(h_minp.data(), 4, bn, f_minp) != bn) st = GB_EINVAL;
+      if (st == GB_OK && f_bits && !bitw.put(h_bits.data(), bn)) st = GB_EINVAL;
+      if (st != GB_OK && W.err.empty() && outputs) W.err = "writing an output file failed";
       if (st != GB_OK) {
         W.st = st;
         W.err = gb_last_error(W.ctx);
@@ -409,6 +536,11 @@ int main(int argc, char** argv) {
     sum.device_ms = std::max(sum.device_ms, w[g].device_ms);
     sum.max_minp = std::max(sum.max_minp, w[g].max_minp);
     if (w[g].first_fail && (!sum.first_fail || w[g].first_fail < sum.first_fail)) sum.first_fail = w[g].first_fail;
+  }
+  if (f_minp) std::fclose(f_minp);
+  if (f_bits) {
+    if (!bitw.finish()) sys_err = true;
+    std::fclose(f_bits);
   }
   for (auto& x : w) gb_destroy(x.ctx);
   if (sys_err) {

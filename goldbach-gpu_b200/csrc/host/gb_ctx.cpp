@@ -729,6 +729,80 @@ gb_status gb_sieve_bitset(gb_ctx* c, uint64_t q_lo, uint64_t nbits, uint32_t* wo
   GB_PUBLIC(c, sieve_bitset_impl(c, c->ws, q_lo, nbits, words, on_device, stream));
 }
 
+// Autotuner: candidates timed on a sample slice at the top of the range
+// (where the sieving primes are largest, so the slice is the range's
+// hardest), through range_impl with no per-n outputs.
+static gb_status autotune_impl(gb_ctx* c, Workspace& w, uint64_t start, uint64_t limit,
+                               const gb_range_opts* base, gb_range_opts* tuned,
+                               gb_autotune_result* res) {
+  if (!tuned) return fail(w, GB_EINVAL, "null tuned");
+  gb_range_opts o{};
+  if (base) o = *base;
+  gb_autotune_result r{};
+  if (limit & 1) limit--;
+  if (start < 4) start = 4;
+  if (start & 1) start++;
+  if (start > limit) return fail(w, GB_EINVAL, "start must be <= limit");
+  const uint64_t count = (limit - start) / 2 + 1;
+  const uint64_t p_small = o.p_small ? o.p_small : 1000000ull;
+  const uint64_t phase2 = o.phase2_limit ? o.phase2_limit : GB_PHASE2_LIMIT_DEFAULT;
+  uint64_t bits = 0;
+  for (uint64_t x = limit; x; x >>= 1) ++bits;
+  const std::vector<uint64_t> key{bits, p_small, phase2};
+  *tuned = o;
+  if (count < (1ull << 22)) {  // too short to be worth timing: the defaults
+    if (res) *res = r;
+    return GB_OK;
+  }
+  auto it = c->tuned.find(key);
+  if (it != c->tuned.end()) {
+    tuned->chunk_evens = it->second.chunk;
+    tuned->halo = it->second.halo;
+    r.chunk_evens = it->second.chunk;
+    r.halo = it->second.halo;
+    r.even_n_per_s = it->second.rate;
+    r.cached = 1;
+    if (res) *res = r;
+    return GB_OK;
+  }
+  const uint64_t sample = std::min<uint64_t>(count, 1ull << 28);
+  const uint64_t s0 = limit - 2 * (sample - 1);
+  gb_range_opts t = o;
+  t.on_device = 0;
+  t.shard_index = 0;
+  t.shard_count = 1;
+  gb_range_result rr{};
+  gb_status st = range_impl(c, w, nullptr, s0, limit, &t, &rr, nullptr);  // warm-up
+  if (st != GB_OK) return st;
+  double best = -1;
+  for (uint32_t chunk : {1u << 18, 1u << 19, 1u << 20})
+    for (uint32_t halo : {1u << 14, 1u << 15, 1u << 16}) {
+      t.chunk_evens = chunk;
+      t.halo = halo;
+      if ((st = range_impl(c, w, nullptr, s0, limit, &t, &rr, nullptr)) != GB_OK) return st;
+      ++r.candidates;
+      const double rate = rr.kernel_ms > 0 ? sample / (rr.kernel_ms / 1e3) : 0;
+      if (rate > best) {
+        best = rate;
+        r.chunk_evens = chunk;
+        r.halo = halo;
+      }
+    }
+  r.even_n_per_s = best;
+  r.sample_evens = sample;
+  c->tuned[key] = gb_ctx::Tuned{r.chunk_evens, r.halo, best};
+  tuned->chunk_evens = r.chunk_evens;
+  tuned->halo = r.halo;
+  if (res) *res = r;
+  return GB_OK;
+}
+
+gb_status gb_autotune_range(gb_ctx* c, uint64_t start, uint64_t limit, const gb_range_opts* base,
+                            gb_range_opts* tuned, gb_autotune_result* res) {
+  if (!c) return GB_EINVAL;
+  GB_PUBLIC(c, autotune_impl(c, c->ws, start, limit, base, tuned, res));
+}
+
 // Partition counts (kernels/counts.cu): the odd-prime bitset of [1, n_max]
 // is sieved into a padded device buffer (two zero words in front, slack
 // behind for the correlation's 64-bit windows), then one warp per 32

@@ -76,6 +76,13 @@ struct gb_ctx {
 
   gb::Workspace ws;  // the public entry points' workspace
   gb_server* server = nullptr;
+  // gb_autotune_range's choices per range class (bit length of the limit,
+  // p_small, phase2_limit) -> (chunk_evens, halo, even n/s)
+  struct Tuned {
+    uint32_t chunk, halo;
+    double rate;
+  };
+  std::map<std::vector<uint64_t>, Tuned> tuned;
 };
 
 namespace gb {

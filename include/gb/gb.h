@@ -142,6 +142,28 @@ gb_status gb_verify_range(gb_ctx* ctx, uint64_t start, uint64_t limit,
                           const gb_range_out* out);
 
 /* -------------------------------------------------------------------------
+ * Autotuner for gb_verify_range (no counterpart in the reference, whose
+ * SEG_SIZE / P_SMALL the user picks by hand, src/goldbach.cu:560-609): times
+ * gb_verify_range on the top min(2^28, count) even n of [start, limit] for
+ * each candidate chunk_evens (2^18, 2^19, 2^20) and halo (2^14, 2^15, 2^16),
+ * after one warm-up call, and writes the fastest into *tuned (a copy of
+ * *base with chunk_evens and halo set).  The choice is cached in the context
+ * per range class (bit length of limit, p_small, phase2_limit): a later call
+ * for the same class times nothing.  Ranges below 2^22 even n keep the
+ * defaults.  Results of gb_verify_range do not depend on these knobs.
+ * ---------------------------------------------------------------------- */
+typedef struct gb_autotune_result {
+  uint32_t chunk_evens;   /* chosen */
+  uint32_t halo;          /* chosen */
+  double even_n_per_s;    /* the chosen configuration's rate on the sample */
+  uint32_t candidates;    /* configurations timed by this call (0: cached) */
+  uint64_t sample_evens;  /* even n per timed call */
+  int cached;             /* 1: the context had this range class */
+} gb_autotune_result;
+gb_status gb_autotune_range(gb_ctx* ctx, uint64_t start, uint64_t limit, const gb_range_opts* base,
+                            gb_range_opts* tuned, gb_autotune_result* res);
+
+/* -------------------------------------------------------------------------
  * Goldbach partition counts: counts[j] = c(n) for n = start + 2j, j < count,
  * where c(n) = #{p <= n/2 : p and n - p prime} (so c(4) = 1, c(6) = 1,
  * c(10) = 2).  Replaces goldbach_count (src/cpu_goldbach.cpp:29-36), the

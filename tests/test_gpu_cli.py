@@ -105,3 +105,30 @@ def test_counts_mode(tmp_path):
     lines = [l for l in out.splitlines() if l.startswith("c(")]
     want = [f"c({g['first_n'] + 2 * j}) = {v}" for j, v in enumerate(g["counts"]) if g["first_n"] + 2 * j <= 2000]
     assert lines == want and "Even numbers counted : 999" in out
+
+
+def test_per_n_output_files(tmp_path, oracle):
+    """--minp-out / --bitmap-out: the minimal p and verified bit of every n,
+    in range order, across segment boundaries that are not byte-aligned."""
+    import numpy as np
+    m, b = tmp_path / "minp.u32", tmp_path / "bits.bin"
+    rc, out = run("goldbach", 2000000, "--seg-size=100002", f"--minp-out={m}", f"--bitmap-out={b}")
+    assert rc == 0, out
+    count = 999999
+    got = np.fromfile(m, np.uint32)
+    np.testing.assert_array_equal(got, oracle.minp(4, count))
+    bits = np.unpackbits(np.fromfile(b, np.uint8), bitorder="little")
+    assert bits.size == (count + 7) // 8 * 8 and bits[:count].all() and not bits[count:].any()
+
+
+def test_autotune_and_its_cache(tmp_path):
+    cache = tmp_path / "tune.txt"
+    args = (4000000000, "--seg-size=67108864", f"--autotune-cache={cache}")
+    rc, out = run("goldbach", *args)
+    assert rc == 0 and "[Autotune] chunk=" in out and "candidates)" in out, out
+    line = cache.read_text().splitlines()[0]
+    assert line.startswith("class 32 1000000 100000000 chunk ")
+    rc, out2 = run("goldbach", *args)
+    assert rc == 0 and f"(from {cache})" in out2
+    ref = [l for l in out.splitlines() if "Phase 2 fallbacks" in l or "satisfy" in l]
+    assert ref == [l for l in out2.splitlines() if "Phase 2 fallbacks" in l or "satisfy" in l]

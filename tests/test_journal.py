@@ -93,3 +93,8 @@ def test_new_journal_gets_a_header(tmp_path):
     j = tmp_path / "j.txt"
     run(*ARGS, f"--journal={j}")
     assert j.read_text().splitlines()[0] == header(4, 1000, 100, 1000)
+
+
+def test_outputs_and_journal_do_not_mix(tmp_path):
+    rc, out = run(1000, f"--minp-out={tmp_path / 'm'}", f"--journal={tmp_path / 'j'}")
+    assert rc == 1 and "cannot be combined with --journal" in out
