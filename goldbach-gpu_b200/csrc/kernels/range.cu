@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(kRangeThreads, 2) range_kernel(const __grid_co
     // window bit i <-> odd index g0 + i, g0 = (A - H) / 2 (negative near 0)
     const int64_t g0 = (int64_t)(c.A >> 1) - (int64_t)(s.halo >> 1);
     const uint32_t nbits = s.halo / 2 + c.cnt + 32;
-    const uint64_t q_top = c.A + 2ull * c.cnt;
+    const uint64_t q_top = c.A + 2ull * (c.cnt - 1);  // the chunk's last n (no wrap below 2^64)
     sieve_window<kRangeThreads>(Q, a.nbw, nbits, g0, q_top, pat, s.primes, a.magic, a.nsieve,
                                 a.kcoop);
     search_chunk<MINP, kRangeThreads>(s, Q, SOFF, HIST, c, &s_fb, &s_maxp, &s_psum);
@@ -153,15 +153,16 @@ __global__ void __launch_bounds__(kRange6Threads, kRange6Blocks) range6_kernel(c
 #pragma unroll
       for (int ri = 0; ri < 3; ++ri) {
         const uint32_t d = (uint32_t)((2 * ri - (int)amod + 6) % 6);
-        cx.n[ri] = A + d;
-        cx.M[ri] = last >= A + d ? (uint32_t)((last - A - d) / 6 + 1) : 0u;
+        cx.n[ri] = A + d;  // (may pass 2^64 only for a class with no n: M = 0)
+        cx.M[ri] = last - A >= d ? (uint32_t)((last - A - d) / 6 + 1) : 0u;
         // K = (X - (p mod 6)) / 6 with X = n_rho - c - 6 G0 (exact)
         cx.K[ri][0] = (a6 + d - 1 - e6_pmod(ri, 0)) / 6;
         cx.K[ri][1] = (a6 + d - 5 - e6_pmod(ri, 1)) / 6;
       }
     }
     const uint32_t nbits = s.halo / 6 + cnt / 3 + 96;
-    sieve_window6<kRange6Threads>(Q1, Q5, a.nbw, nbits, G0, A + 2ull * cnt, pat6, s.primes,
+    // q <= n - 3: the chunk's last n bounds the sieve (A + 2 cnt could pass 2^64)
+    sieve_window6<kRange6Threads>(Q1, Q5, a.nbw, nbits, G0, A + 2ull * (cnt - 1), pat6, s.primes,
                                  a.magic, a.a15, a.nsieve, a.kcoop);
     search_chunk6<MINP, kRange6Threads>(s, surv, a.surv_cap);
   }

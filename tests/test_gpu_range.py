@@ -181,3 +181,20 @@ def test_summary_1e9_matches_oracle_fixture(ctx):
     assert r.result["max_minp"] == g["max_minp"]
     h = {str(i): int(c) for i, c in enumerate(r.hist) if c}
     assert h == g["hist_nonzero"]
+
+
+@pytest.mark.parametrize("count", [1, 2, 3, 97, 1 << 16])
+def test_range_ending_at_the_top_of_uint64(ctx, oracle, count):
+    """Chunks whose last n is 2^64 - 2 (limit 2^64 - 1 normalises to it):
+    sieving primes up to 2^32, and no chunk arithmetic may pass 2^64.
+    Checked against the oracle's single-n search (7-base MR on each q)."""
+    limit = 2**64 - 1
+    start = 2**64 - 2 - 2 * (count - 1)
+    r = ctx.verify_range(start, limit, want_minp=True, want_bits=True)
+    ns = np.array([start + 2 * j for j in range(count)], np.uint64)
+    want = oracle.single_minp(ns, p_limit=10**8).astype(np.uint32)
+    bad = np.nonzero(r.min_p != want)[0]
+    assert bad.size == 0, (ns[bad[:8]], r.min_p[bad[:8]], want[bad[:8]])
+    assert r.result["checked"] == count and r.result["failures"] == 0
+    bits = np.unpackbits(r.verified_bits.view(np.uint8), bitorder="little")
+    assert bits[:count].all()
