@@ -25,7 +25,8 @@ __device__ __forceinline__ uint64_t first_mark(int64_t g0, uint32_t p, uint64_t 
   if (g0 < 0 || (uint64_t)g0 <= gpp) return gpp - (uint64_t)g0;  // start at p^2
   const uint64_t q0 = 2 * (uint64_t)g0 + 1;
   uint32_t r = mod_p(q0, p, magic);
-  uint32_t delta = r ? p - r : 0;  // q0 + delta: first multiple >= q0
+  uint64_t delta = r ? p - r : 0;  // q0 + delta: first multiple >= q0 (64-bit: + p below
+                                   // may pass 2^32 for the primes near 2^32 of q near 2^64)
   if (!(delta & 1)) {              // q0 odd: the multiple is odd iff delta even
   } else {
     delta += p;

@@ -93,8 +93,10 @@ __global__ void __launch_bounds__(kWinThreads) win_tile_kernel(const __grid_cons
     const uint32_t nb = (uint32_t)(d.wbits - b0 < a.tile_bits ? d.wbits - b0 : a.tile_bits);
     const uint32_t nw = nb / 32;  // wbits and tile_bits are multiples of 32
     const int64_t g0 = (int64_t)(d.start >> 1) - (int64_t)(a.s.halo >> 1) + (int64_t)b0;
-    uint64_t q_top = 2 * (uint64_t)(g0 + nb - 1) + 1;
-    if (q_top > d.q_top) q_top = d.q_top;
+    // the tile's top q, or the window's when that is lower (compared in odd
+    // index space: the tile's top may pass 2^64 for windows ending near it)
+    const uint64_t gt = (uint64_t)(g0 + nb - 1);
+    const uint64_t q_top = gt >= (d.q_top >> 1) ? d.q_top : 2 * gt + 1;
     const uint32_t ns = d.nsieve < a.nsmall ? d.nsieve : a.nsmall;
     sieve_window<kWinThreads>(Q, nw, nb, g0, q_top, pat, a.s.primes, a.magic, ns, a.kcoop);
     uint32_t* out = a.bits + d.wbase + b0 / 32;

@@ -59,3 +59,14 @@ def test_is_prime_random_64bit(ctx, oracle):
     got = ctx.is_prime(n)
     want = np.array([oracle.mr7(int(x)) for x in n])
     np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("q_lo,nbits", [(2**64 - 2**21 + 1, 2**20), (2**63 + 1, 100003),
+                                        (2**62 + 2**31 + 1, 65536)])
+def test_sieve_bitset_near_the_top_of_uint64(ctx, q_lo, nbits):
+    """Windows that need sieving primes above 2^31 (q > 2^62) against the
+    device Miller-Rabin (itself checked against the reference's MR)."""
+    bits = ctx.sieve_bitset(q_lo, nbits)
+    got = np.unpackbits(bits.view(np.uint8), bitorder="little")[:nbits].astype(bool)
+    q = q_lo + 2 * np.arange(nbits, dtype=np.uint64)
+    np.testing.assert_array_equal(got, ctx.is_prime(q))

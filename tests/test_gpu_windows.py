@@ -44,3 +44,19 @@ def test_windows_modes_agree_large(ctx):
     b, _, sb = ctx.verify_windows(starts, counts, mode=1)
     assert a == b
     assert sa["failures"] == sb["failures"] == 0
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_windows_at_the_top_of_uint64(ctx, oracle, mode):
+    """Windows ending at 2^64 - 2 and just below it (sieving primes to 2^32),
+    against the oracle's MR-based single-n search."""
+    top = 2**64 - 2
+    counts = np.array([1, 2, 97, 5000], dtype=np.uint64)
+    starts = np.array([top, top - 2, top - 2 * 96 - 10**6, top - 2 * 4999 - 10**9],
+                      dtype=np.uint64)
+    per, minp, _ = ctx.verify_windows(starts, counts, mode=mode, want_minp=True)
+    ns = np.concatenate([s + 2 * np.arange(int(c), dtype=np.uint64) for s, c in zip(starts, counts)])
+    want = oracle.single_minp(ns, p_limit=10**8).astype(np.uint32)
+    bad = np.nonzero(minp != want)[0]
+    assert bad.size == 0, (ns[bad[:8]], minp[bad[:8]], want[bad[:8]])
+    assert all(p["failures"] == 0 for p in per)
