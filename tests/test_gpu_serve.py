@@ -63,3 +63,27 @@ def test_invalid_requests_are_rejected_not_run(gbmod):
         assert r["status"] == 0 and r["p"] + r["q"] == 100 and r["p"] == 3
         assert ctx.serve_stats()["rejected"] == 4
         ctx.serve_stop()
+
+
+def test_high_offsets_match_the_oracle(gbmod, oracle):
+    """Requests near 1e19 and the top of uint64 (both lanes) against the
+    oracle's MR-based minimal-p search."""
+    with gbmod.Context(0, max_n=2**64 - 1) as ctx:
+        ctx.serve_start(max_n=2**64 - 1, small_range=500)
+        rng = np.random.default_rng(5)
+        reqs = [(0, int(rng.integers(5 * 10**17, 2**63 - 1)) * 2, 1) for _ in range(64)]
+        reqs += [(0, 2**64 - 2, 1), (1, 2**64 - 2 - 2 * 99, 100), (1, 2**64 - 2 - 2 * 2999, 3000)]
+        reqs += [(1, int(rng.integers(5 * 10**18, 9 * 10**18)) * 2, int(rng.integers(1, 4000)))
+                 for _ in range(12)]
+        k, a, c = zip(*reqs)
+        got = [ctx.wait(t, 120000) for t in ctx.submit(k, a, c)]
+        assert {g["lane"] for g in got} == {0, 1}
+        for (kind, a0, count), g in zip(reqs, got):
+            ns = np.array([a0 + 2 * j for j in range(count)], np.uint64)
+            m = oracle.single_minp(ns, p_limit=10**8)
+            assert g["status"] == 0
+            if kind == 0:
+                assert g["p"] == int(m[0]) and g["q"] == a0 - int(m[0])
+            assert g["verified"] == int((m > 0).sum()) and g["failures"] == int((m == 0).sum())
+            assert g["max_minp"] == int(m.max()) and g["minp_sum"] == int(m.sum()), (kind, a0, count)
+        ctx.serve_stop()
