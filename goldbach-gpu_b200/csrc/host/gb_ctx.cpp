@@ -91,6 +91,8 @@ gb_status ws_init(gb_ctx* c, Workspace& w, uint32_t queue_cap) {
       (st = dev_alloc(c, (void**)&w.queue, (size_t)queue_cap * sizeof(QEntry), &w.err)) != GB_OK)
     return st;
   w.queue_cap = queue_cap;
+  if (cudaMallocHost((void**)&w.h_stage, (kCtrCount + GB_HIST_BINS) * 8) != cudaSuccess)
+    return fail(w, GB_ENOMEM, "pinned staging buffer");
   if (cudaEventCreate(&w.ev0) != cudaSuccess || cudaEventCreate(&w.ev1) != cudaSuccess ||
       cudaEventCreate(&w.ek0) != cudaSuccess || cudaEventCreate(&w.ek1) != cudaSuccess)
     return fail(w, GB_ECUDA, "cudaEventCreate");
@@ -110,7 +112,29 @@ gb_status ws_scratch(gb_ctx* c, Workspace& w, size_t bytes, void** p) {
   return GB_OK;
 }
 
+gb_status ws_buffer(gb_ctx* c, Workspace& w, Temps& t, int slot, size_t bytes, void** p) {
+  if (t.arena || bytes > kKeptBufferBytes || slot >= Workspace::kBufSlots) return t.get(bytes, p, w);
+  if (bytes > w.buf_bytes[slot]) {
+    dev_free(c, w.buf[slot]);
+    w.buf[slot] = nullptr;
+    w.buf_bytes[slot] = 0;
+    const size_t grow = std::max<size_t>(bytes, 64 << 10);
+    gb_status st = dev_alloc(c, &w.buf[slot], grow, &w.err);
+    if (st != GB_OK) return st;
+    w.buf_bytes[slot] = grow;
+  }
+  *p = w.buf[slot];
+  return GB_OK;
+}
+
 void ws_free(gb_ctx* c, Workspace& w) {
+  for (int i = 0; i < Workspace::kBufSlots; ++i) {
+    dev_free(c, w.buf[i]);
+    w.buf[i] = nullptr;
+    w.buf_bytes[i] = 0;
+  }
+  if (w.h_stage) cudaFreeHost(w.h_stage);
+  w.h_stage = nullptr;
   dev_free(c, w.ctr);
   dev_free(c, w.hist);
   dev_free(c, w.queue);
@@ -361,6 +385,7 @@ gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint
   gb_range_out od{};
   if (out) od = *out;
   Temps tmp(c, arena);
+  int slot = 0;
   auto dev_out = [&](void* user, size_t bytes, void** dptr) -> gb_status {
     *dptr = nullptr;
     if (!user) return GB_OK;
@@ -368,7 +393,7 @@ gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint
       *dptr = user;
       return GB_OK;
     }
-    return tmp.get(bytes, dptr, w);
+    return ws_buffer(c, w, tmp, slot++, bytes, dptr);
   };
   const uint64_t vwords = (count + 31) / 32;
   void *d_vbits, *d_minp, *d_shist, *d_sfb, *d_sfail;
@@ -424,9 +449,11 @@ gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint
   }
   chk(cudaEventRecord(w.ev1, s));
   unsigned long long ctr[kCtrCount];
-  chk(cudaMemcpyAsync(ctr, sp.ctr, sizeof ctr, cudaMemcpyDeviceToHost, s));
-  if (od.minp_hist && !o.on_device)
-    chk(cudaMemcpyAsync(od.minp_hist, sp.hist, GB_HIST_BINS * 8, cudaMemcpyDeviceToHost, s));
+  unsigned long long* st_ctr = w.h_stage;  // pinned: the counters, then the histogram
+  chk(cudaMemcpyAsync(st_ctr, sp.ctr, kCtrCount * 8, cudaMemcpyDeviceToHost, s));
+  const bool hist_host = od.minp_hist && !o.on_device;
+  if (hist_host)
+    chk(cudaMemcpyAsync(st_ctr + kCtrCount, sp.hist, GB_HIST_BINS * 8, cudaMemcpyDeviceToHost, s));
   if (!o.on_device) {
     if (od.verified_bits) chk(cudaMemcpyAsync(od.verified_bits, sp.vbits, vwords * 4, cudaMemcpyDeviceToHost, s));
     if (od.min_p) chk(cudaMemcpyAsync(od.min_p, sp.minp, count * 4, cudaMemcpyDeviceToHost, s));
@@ -435,6 +462,8 @@ gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint
     if (od.seg_failures) chk(cudaMemcpyAsync(od.seg_failures, sp.unit_failures, nseg * 4, cudaMemcpyDeviceToHost, s));
   }
   chk(cudaStreamSynchronize(s));
+  std::memcpy(ctr, st_ctr, sizeof ctr);
+  if (hist_host && e == cudaSuccess) std::memcpy(od.minp_hist, st_ctr + kCtrCount, GB_HIST_BINS * 8);
   float ms = 0, kms = 0;
   if (e == cudaSuccess) {
     cudaEventElapsedTime(&ms, w.ev0, w.ev1);
@@ -481,7 +510,7 @@ gb_status single_impl(gb_ctx* c, Workspace& w, Arena* arena, const uint64_t* n, 
   Temps tmp(c, arena);
   if (!o.on_device && count) {
     void* t;
-    if ((st = tmp.get(count * 8 * 3, &t, w)) != GB_OK) return st;
+    if ((st = ws_buffer(c, w, tmp, 0, count * 8 * 3, &t)) != GB_OK) return st;
     dn = (const uint64_t*)t;
     dp = (uint64_t*)t + count;
     dq = (uint64_t*)t + 2 * count;
@@ -701,7 +730,7 @@ static gb_status sieve_bitset_impl(gb_ctx* c, Workspace& w, uint64_t q_lo, uint6
   Temps tmp(c, nullptr);
   uint32_t* d = words;
   const uint64_t nwords = (nbits + 31) / 32;
-  if (!on_device && (st = tmp.get(nwords * 4, (void**)&d, w)) != GB_OK) return st;
+  if (!on_device && (st = ws_buffer(c, w, tmp, 0, nwords * 4, (void**)&d)) != GB_OK) return st;
   const uint32_t tile = 1u << 18;
   uint64_t ns = 0, kc = 0;
   if ((st = count_le(c, w, root, &ns)) != GB_OK || (st = count_le(c, w, tile / 64, &kc)) != GB_OK)
@@ -826,8 +855,8 @@ static gb_status counts_impl(gb_ctx* c, Workspace& w, uint64_t start, uint64_t c
   Temps tmp(c, nullptr);
   uint32_t* buf = nullptr;
   unsigned long long* d_out = (unsigned long long*)counts;
-  if ((st = tmp.get((nwords + 8) * 4, (void**)&buf, w)) != GB_OK) return st;
-  if (!o.on_device && (st = tmp.get(count * 8, (void**)&d_out, w)) != GB_OK) return st;
+  if ((st = ws_buffer(c, w, tmp, 0, (nwords + 8) * 4, (void**)&buf)) != GB_OK) return st;
+  if (!o.on_device && (st = ws_buffer(c, w, tmp, 1, count * 8, (void**)&d_out)) != GB_OK) return st;
   const uint32_t tile = 1u << 18;
   const uint64_t root = isqrt_u64(n_max);
   uint64_t ns = 0, kc = 0;
@@ -897,7 +926,8 @@ static gb_status is_prime_impl(gb_ctx* c, Workspace& w, const uint64_t* n, size_
   Temps tmp(c, nullptr);
   gb_status st;
   if (!on_device) {
-    if ((st = tmp.get(count * 8, (void**)&dn, w)) != GB_OK || (st = tmp.get(count, (void**)&dout, w)) != GB_OK)
+    if ((st = ws_buffer(c, w, tmp, 0, count * 8, (void**)&dn)) != GB_OK ||
+        (st = ws_buffer(c, w, tmp, 1, count, (void**)&dout)) != GB_OK)
       return st;
   }
   cudaError_t e = cudaSuccess;

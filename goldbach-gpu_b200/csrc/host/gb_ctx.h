@@ -47,6 +47,13 @@ struct Workspace {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ek0 = nullptr, ek1 = nullptr;
   void* scratch = nullptr;  // per-call kernel scratch, grown on demand
   size_t scratch_bytes = 0;
+  // per-call device buffers of the public entry points (slot i grown on
+  // demand and kept, up to kKeptBufferBytes; larger ones are per call)
+  static constexpr int kBufSlots = 8;
+  void* buf[kBufSlots] = {};
+  size_t buf_bytes[kBufSlots] = {};
+  // pinned staging for the counters and the histogram read back by each call
+  unsigned long long* h_stage = nullptr;  // kCtrCount + GB_HIST_BINS
   std::string err;
 };
 
@@ -103,6 +110,12 @@ gb_status ws_init(gb_ctx* c, Workspace& w, uint32_t queue_cap);
 void ws_free(gb_ctx* c, Workspace& w);
 // The workspace's scratch buffer, grown to at least `bytes`.
 gb_status ws_scratch(gb_ctx* c, Workspace& w, size_t bytes, void** p);
+// Per-call device buffers kept between calls (no cudaMalloc / cudaFree per
+// call for the usual sizes): slot `slot` of the workspace, grown to `bytes`;
+// above kKeptBufferBytes the buffer comes from `t` and is freed with it.
+constexpr size_t kKeptBufferBytes = 256ull << 20;
+struct Temps;
+gb_status ws_buffer(gb_ctx* c, Workspace& w, Temps& t, int slot, size_t bytes, void** p);
 gb_status ensure_primes(gb_ctx* c, Workspace& w, uint64_t limit);
 // number of primes <= x in the resident table (x <= primes_limit)
 gb_status count_le(gb_ctx* c, Workspace& w, uint64_t x, uint64_t* out);

@@ -89,14 +89,14 @@ gb_status windows_impl(gb_ctx* c, Workspace& ws, Arena* arena, const gb_window* 
 
   Temps tmp(c, arena);
   void *d_desc, *d_toff, *d_coff, *d_bits, *d_fail, *d_maxp, *d_psum, *d_minp = nullptr;
-  if ((st = tmp.get(count * sizeof(WinDesc), &d_desc, ws)) != GB_OK ||
-      (st = tmp.get((count + 1) * 8, &d_toff, ws)) != GB_OK ||
-      (st = tmp.get((count + 1) * 8, &d_coff, ws)) != GB_OK ||
-      (st = tmp.get(words * 4, &d_bits, ws)) != GB_OK ||
-      (st = tmp.get(count * 4, &d_fail, ws)) != GB_OK ||
-      (st = tmp.get(count * 8, &d_maxp, ws)) != GB_OK ||
-      (st = tmp.get(count * 8, &d_psum, ws)) != GB_OK ||
-      (min_p_concat && (st = tmp.get(total_n * 4, &d_minp, ws)) != GB_OK))
+  if ((st = ws_buffer(c, ws, tmp, 0, count * sizeof(WinDesc), &d_desc)) != GB_OK ||
+      (st = ws_buffer(c, ws, tmp, 1, (count + 1) * 8, &d_toff)) != GB_OK ||
+      (st = ws_buffer(c, ws, tmp, 2, (count + 1) * 8, &d_coff)) != GB_OK ||
+      (st = ws_buffer(c, ws, tmp, 3, words * 4, &d_bits)) != GB_OK ||
+      (st = ws_buffer(c, ws, tmp, 4, count * 4, &d_fail)) != GB_OK ||
+      (st = ws_buffer(c, ws, tmp, 5, count * 8, &d_maxp)) != GB_OK ||
+      (st = ws_buffer(c, ws, tmp, 6, count * 8, &d_psum)) != GB_OK ||
+      (min_p_concat && (st = ws_buffer(c, ws, tmp, 7, total_n * 4, &d_minp)) != GB_OK))
     return st;
   WindowsArgs a{};
   SearchParams& sp = a.s;
