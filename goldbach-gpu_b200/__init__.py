@@ -88,7 +88,7 @@ class Window(C.Structure):
 
 class WindowsOpts(C.Structure):
     _fields_ = [("mode", i32), ("chunk_evens", u32), ("halo", u32),
-                ("phase2_limit", u64), ("on_device", i32), ("stream", vp)]
+                ("phase2_limit", u64), ("on_device", i32), ("stream", vp), ("mr_below", u64)]
 
 
 class WindowResult(C.Structure):
@@ -349,7 +349,7 @@ class Context:
 
     # -- windows -------------------------------------------------------------
     def verify_windows(self, starts, counts, *, mode=GB_WINDOWS_PERSISTENT, chunk=0, halo=0,
-                       phase2_limit=0, want_minp=False, stream=None):
+                       phase2_limit=0, want_minp=False, stream=None, mr_below=0):
         starts = np.asarray(starts, dtype=np.uint64)
         counts = np.asarray(counts, dtype=np.uint64)
         nw = len(starts)
@@ -360,7 +360,7 @@ class Context:
         res = (WindowResult * nw)()
         minp = np.zeros(int(counts.sum()), np.uint32) if want_minp else None
         s = WindowsSummary()
-        o = WindowsOpts(mode, chunk, halo, phase2_limit, 0, stream or None)
+        o = WindowsOpts(mode, chunk, halo, phase2_limit, 0, stream or None, mr_below)
         self._check(self.L.gb_verify_windows(self._h, w, nw, C.byref(o), res,
                                              _ptr(minp), C.byref(s)))
         per = [{f: getattr(res[i], f) for f, _ in WindowResult._fields_} for i in range(nw)]

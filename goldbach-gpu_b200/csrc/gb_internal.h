@@ -5,6 +5,8 @@
 
 #include <cstdint>
 
+#include "gb/gb.h"
+
 namespace gb {
 
 // Global counters of a call (device array of unsigned long long).
@@ -160,6 +162,8 @@ struct SingleArgs {
 };
 cudaError_t launch_single(const SingleArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_is_prime(const uint64_t* n, uint64_t count, uint8_t* out, cudaStream_t s);
+cudaError_t launch_win_expand(const gb_window* w, const uint64_t* off, uint32_t nw, uint64_t* n,
+                              cudaStream_t s);
 cudaError_t launch_segment_reduce(const uint64_t* p, const uint64_t* off, uint32_t nreq,
                                   unsigned long long* agg, cudaStream_t s);
 

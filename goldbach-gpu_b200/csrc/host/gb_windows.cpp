@@ -8,8 +8,10 @@
 // runs the same stages window by window with per-window grids (the plain
 // per-window pipeline, kept for comparison).
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <numeric>
+#include <vector>
 
 #include "gb_ctx.h"
 
@@ -20,9 +22,10 @@ constexpr uint64_t kWinSmallPrimeBound = 1ull << 17;  // tile sieve marks primes
 
 namespace gb {
 
-gb_status windows_impl(gb_ctx* c, Workspace& ws, Arena* arena, const gb_window* w, size_t count,
-                       const gb_windows_opts* opts, gb_window_result* res, uint32_t* min_p_concat,
-                       gb_windows_summary* sum) {
+// The sieve pipeline over windows w[0..count) (stages of kernels/windows.cu).
+static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, const gb_window* w,
+                                    size_t count, const gb_windows_opts* opts, gb_window_result* res,
+                                    uint32_t* min_p_concat, gb_windows_summary* sum) {
   if (count && !w) return fail(ws, GB_EINVAL, "null windows");
   gb_windows_opts o{};
   if (opts) o = *opts;
@@ -196,6 +199,162 @@ gb_status windows_impl(gb_ctx* c, Workspace& ws, Arena* arena, const gb_window* 
     sum->failures = ctr[kCtrFailures];
     sum->kernel_launches = launches;
     sum->device_ms = ms;
+  }
+  return GB_OK;
+}
+
+
+// Narrow windows on the Miller-Rabin path: every n of every window through
+// the single-n kernel (minimal p over the resident table, q by the 7-base
+// MR), then one per-window reduction.  Plain mode launches the single-n
+// kernel window by window.
+static gb_status windows_mr_impl(gb_ctx* c, Workspace& ws, Arena* arena, const gb_window* w,
+                                 size_t count, const gb_windows_opts& o, uint64_t p_lim,
+                                 gb_window_result* res, uint32_t* min_p_concat,
+                                 gb_windows_summary* sum) {
+  uint64_t total = 0;
+  std::vector<uint64_t> off(count + 1, 0);
+  for (size_t i = 0; i < count; ++i) off[i + 1] = off[i] + w[i].count;
+  total = off[count];
+  uint64_t np = 0;
+  gb_status st = count_le(c, ws, p_lim, &np);
+  if (st != GB_OK) return st;
+  Temps tmp(c, arena);
+  void *d_w, *d_off, *d_n, *d_p, *d_q, *d_agg;
+  if ((st = tmp.get(count * sizeof(gb_window), &d_w, ws)) != GB_OK ||
+      (st = tmp.get((count + 1) * 8, &d_off, ws)) != GB_OK ||
+      (st = tmp.get(total * 8, &d_n, ws)) != GB_OK || (st = tmp.get(total * 8, &d_p, ws)) != GB_OK ||
+      (st = tmp.get(total * 8, &d_q, ws)) != GB_OK || (st = tmp.get(count * 32, &d_agg, ws)) != GB_OK)
+    return st;
+  cudaStream_t s = o.stream ? (cudaStream_t)o.stream : c->stream;
+  cudaError_t e = cudaSuccess;
+  auto chk = [&](cudaError_t x) {
+    if (e == cudaSuccess && x != cudaSuccess) e = x;
+  };
+  int launches = 0;
+  chk(cudaEventRecord(ws.ev0, s));
+  chk(cudaMemcpyAsync(d_w, w, count * sizeof(gb_window), cudaMemcpyHostToDevice, s));
+  chk(cudaMemcpyAsync(d_off, off.data(), (count + 1) * 8, cudaMemcpyHostToDevice, s));
+  chk(launch_win_expand((const gb_window*)d_w, (const uint64_t*)d_off, (uint32_t)count, (uint64_t*)d_n, s));
+  ++launches;
+  SingleArgs a{};
+  a.primes = c->d_primes;
+  a.nprimes = np;
+  a.p_lim = p_lim;
+  a.ctr = ws.ctr;
+  const size_t parts = o.mode == GB_WINDOWS_PLAIN ? count : 1;
+  for (size_t i = 0; i < parts && e == cudaSuccess; ++i) {
+    const uint64_t b = parts == 1 ? 0 : off[i], n = parts == 1 ? total : w[i].count;
+    a.n = (const uint64_t*)d_n + b;
+    a.count = n;
+    a.p_out = (uint64_t*)d_p + b;
+    a.q_out = (uint64_t*)d_q + b;
+    chk(cudaMemsetAsync(ws.ctr, 0, 4 * 8, s));
+    const uint64_t grid = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)c->sm_count * 6, (n + 7) / 8));
+    chk(launch_single(a, (int)grid, s));
+    ++launches;
+  }
+  chk(launch_segment_reduce((const uint64_t*)d_p, (const uint64_t*)d_off, (uint32_t)count,
+                            (unsigned long long*)d_agg, s));
+  ++launches;
+  chk(cudaEventRecord(ws.ev1, s));
+  std::vector<unsigned long long> agg(count * 4);
+  std::vector<uint64_t> pv(min_p_concat ? total : 0);
+  chk(cudaMemcpyAsync(agg.data(), d_agg, count * 32, cudaMemcpyDeviceToHost, s));
+  if (min_p_concat) chk(cudaMemcpyAsync(pv.data(), d_p, total * 8, cudaMemcpyDeviceToHost, s));
+  chk(cudaStreamSynchronize(s));
+  if (e != cudaSuccess) return cuda_fail(ws, e, "windows (Miller-Rabin path)");
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ws.ev0, ws.ev1);
+  uint64_t fails = 0;
+  for (size_t i = 0; i < count; ++i) {
+    if (res) {
+      res[i].verified = agg[4 * i];
+      res[i].failures = agg[4 * i + 1];
+      res[i].max_minp = agg[4 * i + 2];
+      res[i].minp_sum = agg[4 * i + 3];
+    }
+    fails += agg[4 * i + 1];
+  }
+  for (uint64_t j = 0; j < pv.size(); ++j) min_p_concat[j] = (uint32_t)pv[j];
+  if (sum) {
+    sum->total_n = total;
+    sum->failures = fails;
+    sum->kernel_launches = launches;
+    sum->device_ms = ms;
+  }
+  return GB_OK;
+}
+
+// Splits the batch, trading the sieve bound against Miller-Rabin: windows
+// narrower than the sieve's break-even take the Miller-Rabin path (the
+// sieve's large-prime pass costs about 2.5 ps of GPU time per sieving prime
+// per window, the single-n path about 13 ns per n, so the break-even width
+// is about pi(sqrt(top)) / 5300 even n).  Results do not depend on the split.
+gb_status windows_impl(gb_ctx* c, Workspace& ws, Arena* arena, const gb_window* w, size_t count,
+                       const gb_windows_opts* opts, gb_window_result* res, uint32_t* min_p_concat,
+                       gb_windows_summary* sum) {
+  gb_windows_opts o{};
+  if (opts) o = *opts;
+  if (!count || !w || o.on_device || o.mr_below == 1 ||
+      (o.mode != GB_WINDOWS_PERSISTENT && o.mode != GB_WINDOWS_PLAIN))
+    return windows_sieve_impl(c, ws, arena, w, count, opts, res, min_p_concat, sum);
+  std::vector<char> narrow(count, 0);
+  size_t nn = 0;
+  for (size_t i = 0; i < count; ++i) {
+    const uint64_t last = w[i].start + 2 * (w[i].count - 1);
+    if (w[i].start < 4 || (w[i].start & 1) || w[i].count == 0 || last < w[i].start)
+      return windows_sieve_impl(c, ws, arena, w, count, opts, res, min_p_concat, sum);  // reports it
+    uint64_t lim = o.mr_below;
+    if (!lim) {
+      const double r = std::sqrt((double)last);
+      lim = r > 1e4 ? (uint64_t)(1.1 * r / std::log(r) / 5300.0) : 0;
+    }
+    narrow[i] = w[i].count < lim;
+    nn += narrow[i];
+  }
+  if (nn == 0) return windows_sieve_impl(c, ws, arena, w, count, opts, res, min_p_concat, sum);
+  const uint64_t p_lim = o.phase2_limit ? o.phase2_limit : GB_PHASE2_LIMIT_DEFAULT;
+  if (p_lim > GB_P_SMALL_MAX) return fail(ws, GB_EINVAL, "phase2_limit must be <= 4e9");
+  gb_status st = ensure_primes(c, ws, std::max<uint64_t>(p_lim, kWinSmallPrimeBound));
+  if (st != GB_OK) return st;
+  // both parts in their own arrays, results put back in the caller's order
+  std::vector<gb_window> wa, wb;
+  std::vector<size_t> ia, ib;
+  std::vector<uint64_t> out_off(count + 1, 0);
+  for (size_t i = 0; i < count; ++i) {
+    out_off[i + 1] = out_off[i] + w[i].count;
+    (narrow[i] ? wa : wb).push_back(w[i]);
+    (narrow[i] ? ia : ib).push_back(i);
+  }
+  std::vector<gb_window_result> ra(wa.size()), rb(wb.size());
+  uint64_t na = 0, nb = 0;
+  for (const gb_window& x : wa) na += x.count;
+  for (const gb_window& x : wb) nb += x.count;
+  std::vector<uint32_t> ma(min_p_concat ? na : 0), mb(min_p_concat ? nb : 0);
+  gb_windows_summary sa{}, sb{};
+  if ((st = windows_mr_impl(c, ws, arena, wa.data(), wa.size(), o, p_lim, ra.data(),
+                            min_p_concat ? ma.data() : nullptr, &sa)) != GB_OK)
+    return st;
+  if (!wb.empty() && (st = windows_sieve_impl(c, ws, arena, wb.data(), wb.size(), &o, rb.data(),
+                                              min_p_concat ? mb.data() : nullptr, &sb)) != GB_OK)
+    return st;
+  uint64_t pa = 0, pb = 0;
+  for (size_t k = 0; k < ia.size(); ++k) {
+    if (res) res[ia[k]] = ra[k];
+    if (min_p_concat) std::memcpy(min_p_concat + out_off[ia[k]], ma.data() + pa, wa[k].count * 4);
+    pa += wa[k].count;
+  }
+  for (size_t k = 0; k < ib.size(); ++k) {
+    if (res) res[ib[k]] = rb[k];
+    if (min_p_concat) std::memcpy(min_p_concat + out_off[ib[k]], mb.data() + pb, wb[k].count * 4);
+    pb += wb[k].count;
+  }
+  if (sum) {
+    sum->total_n = sa.total_n + sb.total_n;
+    sum->failures = sa.failures + sb.failures;
+    sum->kernel_launches = sa.kernel_launches + sb.kernel_launches;
+    sum->device_ms = sa.device_ms + sb.device_ms;
   }
   return GB_OK;
 }

@@ -185,6 +185,23 @@ __global__ void __launch_bounds__(kWinThreads, 2) win_search_kernel(const __grid
   }
 }
 
+// D. narrow windows on the Miller-Rabin path: the n of each window, laid out
+// window after window at off[i], for the single-n kernel -------------------
+__global__ void win_expand_kernel(const gb_window* __restrict__ w, const uint64_t* __restrict__ off,
+                                  uint32_t nw, uint64_t* __restrict__ n) {
+  for (uint32_t i = blockIdx.x; i < nw; i += gridDim.x) {
+    const uint64_t s = w[i].start, c = w[i].count, o = off[i];
+    for (uint64_t j = threadIdx.x; j < c; j += blockDim.x) n[o + j] = s + 2 * j;
+  }
+}
+
+cudaError_t launch_win_expand(const gb_window* w, const uint64_t* off, uint32_t nw, uint64_t* n,
+                              cudaStream_t s) {
+  if (!nw) return cudaSuccess;
+  win_expand_kernel<<<nw < 4096 ? nw : 4096, 256, 0, s>>>(w, off, nw, n);
+  return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 static size_t tile_smem(const WindowsArgs& a) {
   return (size_t)(kWheelWords + a.tile_bits / 32 + 2) * sizeof(uint32_t);

@@ -271,6 +271,11 @@ typedef struct gb_windows_opts {
   uint64_t phase2_limit;  /* 0: 1e8                                         */
   int on_device;          /* windows / min_p / res are device pointers      */
   void* stream;
+  uint64_t mr_below;      /* windows of fewer even n skip the sieve: their q
+                             are tested by Miller-Rabin (the single-n
+                             kernel).  0: automatic, where sieving would
+                             cost more (about pi(sqrt(top)) / 5300 n);
+                             1: never                                      */
 } gb_windows_opts;
 
 typedef struct gb_window_result {

@@ -60,3 +60,22 @@ def test_windows_at_the_top_of_uint64(ctx, oracle, mode):
     bad = np.nonzero(minp != want)[0]
     assert bad.size == 0, (ns[bad[:8]], minp[bad[:8]], want[bad[:8]])
     assert all(p["failures"] == 0 for p in per)
+
+
+@pytest.mark.parametrize("mr_below", [1, 1 << 40])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_sieve_and_miller_rabin_paths_agree(ctx, oracle, mr_below, mode):
+    """mr_below = 1: every window sieved; 2^40: every window on the
+    Miller-Rabin path; the default splits by width.  Same minimal p."""
+    starts, counts = seeded_windows(7, 24, wmin=10, wmax=13)
+    per, minp, summ = ctx.verify_windows(starts, counts, mode=mode, want_minp=True,
+                                         mr_below=mr_below)
+    want = oracle.minp_windows(starts, counts)
+    np.testing.assert_array_equal(minp, want)
+    off = 0
+    for i, c in enumerate(counts):
+        w = want[off:off + int(c)]
+        assert per[i]["verified"] == c and per[i]["failures"] == 0
+        assert per[i]["max_minp"] == int(w.max()) and per[i]["minp_sum"] == int(w.astype(np.uint64).sum())
+        off += int(c)
+    assert summ["total_n"] == int(counts.sum())
