@@ -351,9 +351,20 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--ref-sample-log2", type=int, default=24)
+    ap.add_argument("--extra", choices=["windows", "single", "counts", "serving"],
+                    help="run only this secondary measurement and print its JSON (profiling)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.extra:
+        gb = load_gb()
+        if args.extra == "serving":
+            print(json.dumps(measure_serving(gb, 0)))
+        else:
+            with gb.Context(0) as c:
+                f = {"windows": measure_windows, "single": measure_single, "counts": measure_counts}
+                print(json.dumps(f[args.extra](gb, c)))
+        return 0
 
     import torch
 
