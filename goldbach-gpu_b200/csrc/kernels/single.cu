@@ -4,16 +4,25 @@
 // 95-282).  The reference sieves p in chunks of 1e8 on the CPU, copies them
 // to the GPU, runs one thread per p with a 128-bit-remainder Miller-Rabin
 // and keeps whichever thread finishes first, so its p is not the minimal
-// one.  Here one warp serves one query n from a device work counter (query
-// cost is uneven):
-//   1. lanes take 32 consecutive primes p from the resident table and drop
-//      those with q = n - p divisible by a prime r <= 61, using
-//      q == 0 (mod r)  <=>  n mod r == p mod r  (n mod r computed once);
-//   2. survivors are gathered in order until 32 are pending, then each lane
-//      runs the base-2 strong test on one of them (Montgomery, 64-bit);
-//   3. the lowest lane that passed gets the other six bases of the
-//      deterministic set, one base per lane; if all pass, its p is the
-//      minimal p (every smaller candidate was rejected above).
+// one.  Here every lane of a warp owns one query n (taken from a device work
+// counter as it frees up) and walks the candidate primes p = 3, 5, 7, ...
+// in order until q = n - p is prime:
+//   1. candidates come in batches of 32 consecutive primes, filtered by the
+//      whole warp for the query that needs them (lane i tests the i-th
+//      prime): q is dropped when a prime r <= 61 divides it, tested on
+//      x = q mod M for three products M of those primes (x = n mod M - p
+//      mod M, n mod M computed once per query) by exact-division checks;
+//   2. each lane runs one strong probable-prime test per round on its own
+//      next survivor: base 2 first, then, for a base-2 pass, the six other
+//      bases of the deterministic set one per round, so a query takes about
+//      12 rounds (about 5.7 base-2 tests for n near 2^63) and every lane
+//      does useful work in every round;
+//   3. a round's exponentiation is uniform across the warp: a fixed 2-bit
+//      window (squaring twice, then one product with 1, a, a^2 or a^3 picked
+//      by the two exponent bits) over the warp's longest exponent, so lanes
+//      with different q and bases never diverge.
+// Queries n < 2^21 (where q may be a prime <= 61) take a warp-cooperative
+// scan with the full test per candidate instead.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -24,8 +33,8 @@
 namespace gb {
 
 constexpr int kSingleThreads = 256;
-constexpr int kSingleWarps = kSingleThreads / 32;
 constexpr uint64_t kSmallN = 1ull << 21;  // below this, q may be tiny: plain path
+constexpr uint32_t kFull = 0xffffffffu;
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
   uint32_t m;
@@ -33,116 +42,224 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
   return m;
 }
 
-// Lane-parallel ascending scan with the full primality test per lane.
-__device__ uint32_t minp_plain(const SingleArgs& a, uint64_t n) {
+// Lane-parallel ascending scan with the full primality test per lane (the
+// whole warp serves one n).
+__device__ uint32_t minp_plain(const SingleArgs& a, uint64_t n, uint64_t lim) {
   const int lane = threadIdx.x & 31;
-  const uint64_t half = n >> 1;
-  const uint64_t lim = half < a.p_lim ? half : a.p_lim;
   for (uint64_t k = 1;; k += 32) {
     const uint64_t kk = k + lane;
     const uint32_t p = kk < a.nprimes ? a.primes[kk] : 0xffffffffu;
     const bool valid = kk < a.nprimes && p <= lim;
     const bool ok = valid && is_prime_u64(n - p);
-    const uint32_t b = __ballot_sync(0xffffffffu, ok);
-    if (b) return __shfl_sync(0xffffffffu, p, __ffs(b) - 1);
-    if (__ballot_sync(0xffffffffu, valid) != 0xffffffffu) return 0;
+    const uint32_t b = __ballot_sync(kFull, ok);
+    if (b) return __shfl_sync(kFull, p, __ffs(b) - 1);
+    if (__ballot_sync(kFull, valid) != kFull) return 0;
   }
 }
 
-#define GB_SMALL_PRIMES(X) \
-  X(3) X(5) X(7) X(11) X(13) X(17) X(19) X(23) X(29) X(31) X(37) X(41) X(43) X(47) X(53) X(59) X(61)
+// Exact division by an odd r on 32-bit x: x * r^-1 (mod 2^32) lands in
+// [0, (2^32-1)/r] exactly for the multiples of r.
+__host__ __device__ constexpr uint32_t inv32(uint32_t r) {
+  uint32_t x = r;  // r*r == 1 (mod 8)
+  for (int i = 0; i < 4; ++i) x *= 2u - r * x;
+  return x;
+}
+template <uint32_t R>
+__device__ __forceinline__ bool divides(uint32_t x) {
+  constexpr uint32_t kInv = inv32(R), kLim = 0xffffffffu / R;
+  static_assert(R * kInv == 1u, "inverse");
+  return x * kInv <= kLim;
+}
 
-__device__ uint32_t minp_big(const SingleArgs& a, uint64_t n, uint32_t* buf) {
-  const int lane = threadIdx.x & 31;
-  const uint64_t half = n >> 1;
-  const uint64_t lim = half < a.p_lim ? half : a.p_lim;
-#define GB_NMOD(r) const uint32_t nm##r = (uint32_t)(n % r##u);
-  GB_SMALL_PRIMES(GB_NMOD)
-#undef GB_NMOD
-  uint64_t k = 1;
-  uint32_t nsurv = 0;
-  bool exhausted = false;
-  for (;;) {
-    while (nsurv < 32 && !exhausted) {
-      const uint64_t kk = k + lane;
-      const uint32_t p = kk < a.nprimes ? a.primes[kk] : 0xffffffffu;
-      const bool valid = kk < a.nprimes && p <= lim;
-      bool pass = valid;
-#define GB_SIEVE(r) pass = pass && (p % r##u != nm##r);
-      GB_SMALL_PRIMES(GB_SIEVE)
-#undef GB_SIEVE
-      const uint32_t b = __ballot_sync(0xffffffffu, pass);
-      if (pass) buf[nsurv + __popc(b & lanemask_lt())] = (uint32_t)kk;
-      nsurv += __popc(b);
-      if (__ballot_sync(0xffffffffu, valid) != 0xffffffffu) exhausted = true;
-      k += 32;
-    }
-    __syncwarp();
-    if (nsurv == 0) return 0;
-    const uint32_t take = nsurv < 32 ? nsurv : 32;
-    bool ok2 = false;
-    uint64_t q = 0;
-    uint32_t pk = 0;
-    if (lane < (int)take) {
-      pk = a.primes[buf[lane]];
-      q = n - pk;
-      uint64_t d = q - 1;
-      const int s = __ffsll((long long)d) - 1;
-      d >>= s;
-      const Mont M = mont_init(q);
-      ok2 = sprp2(M, d, s);
-    }
-    uint32_t b = __ballot_sync(0xffffffffu, ok2);
-    while (b) {
-      const int l = __ffs(b) - 1;
-      const uint64_t qc = __shfl_sync(0xffffffffu, q, l);
-      const uint32_t pc = __shfl_sync(0xffffffffu, pk, l);
-      bool ok = true;
-      if (lane < 6) {
-        uint64_t d = qc - 1;
-        const int s = __ffsll((long long)d) - 1;
-        d >>= s;
-        const Mont M = mont_init(qc);
-        ok = sprp_base_k(M, mont_r2(M), lane + 1, d, s);
-      }
-      if (__all_sync(0xffffffffu, ok)) return pc;
-      b &= b - 1;
-    }
-    // none of the first `take` survivors is prime: drop them
-    __syncwarp();
-    uint32_t keep = 0;
-    if (lane + take < nsurv) keep = buf[lane + take];
-    __syncwarp();
-    if (lane + take < nsurv) buf[lane] = keep;
-    __syncwarp();
-    nsurv -= take;
+constexpr uint32_t kM1 = 3u * 5 * 7 * 11 * 13 * 17 * 19 * 23;  // 111546435
+constexpr uint32_t kM2 = 29u * 31 * 37 * 41 * 43;              // 58642669
+constexpr uint32_t kM3 = 47u * 53 * 59 * 61;                   // 8965109
+
+// q = n - p has no prime factor <= 61, from n mod M1, M2, M3.
+__device__ __forceinline__ bool no_small_factor(uint32_t nm1, uint32_t nm2, uint32_t nm3,
+                                                uint32_t p) {
+  uint32_t x = nm1 + kM1 - p % kM1;
+  x = x >= kM1 ? x - kM1 : x;
+  bool f = divides<3>(x) | divides<5>(x) | divides<7>(x) | divides<11>(x) | divides<13>(x) |
+           divides<17>(x) | divides<19>(x) | divides<23>(x);
+  uint32_t y = nm2 + kM2 - p % kM2;
+  y = y >= kM2 ? y - kM2 : y;
+  f |= divides<29>(y) | divides<31>(y) | divides<37>(y) | divides<41>(y) | divides<43>(y);
+  uint32_t z = nm3 + kM3 - p % kM3;
+  z = z >= kM3 ? z - kM3 : z;
+  f |= divides<47>(z) | divides<53>(z) | divides<59>(z) | divides<61>(z);
+  return !f;
+}
+
+// Strong probable-prime test of every lane's odd modulus M.n = d 2^s + 1 to
+// its base a1 (Montgomery form), the loop lengths set by the warp's longest
+// exponent and largest s (lanes with act false only run along).
+__device__ __forceinline__ bool sprp_warp(const Mont& M, uint64_t a1, uint64_t d, int s, bool act) {
+  const uint64_t a2 = mont_mul(a1, a1, M);
+  const uint64_t a3 = mont_mul(a2, a1, M);
+  const int top = 63 - __clzll(d);  // d >= 1
+  const int T = (int)__reduce_max_sync(kFull, act ? (uint32_t)top : 0u) | 1;  // odd
+  // bit pairs (i+1, i) from i = T-1 down to 0; the first pair starts x
+  uint32_t b = (uint32_t)(d >> (T - 1)) & 3u;
+  uint64_t x = b == 0 ? M.one : b == 1 ? a1 : b == 2 ? a2 : a3;
+  for (int i = T - 3; i >= 0; i -= 2) {
+    x = mont_mul(x, x, M);
+    x = mont_mul(x, x, M);
+    b = (uint32_t)(d >> i) & 3u;
+    x = mont_mul(x, b == 0 ? M.one : b == 1 ? a1 : b == 2 ? a2 : a3, M);
   }
+  const uint64_t mone = M.n - M.one;
+  bool ok = x == M.one || x == mone;
+  bool done = ok;
+  const int S = (int)__reduce_max_sync(kFull, act ? (uint32_t)s : 0u);
+  for (int i = 1; i < S; ++i) {
+    x = mont_mul(x, x, M);
+    if (!done && i < s) {
+      if (x == mone) ok = done = true;
+      else if (x == M.one) done = true;
+    }
+  }
+  return ok;
 }
 
 __global__ void __launch_bounds__(kSingleThreads) single_kernel(SingleArgs a) {
-  __shared__ uint32_t sbuf[kSingleWarps][64];
   const int lane = threadIdx.x & 31;
-  uint32_t* buf = sbuf[threadIdx.x >> 5];
-  for (;;) {
-    unsigned long long qi = 0;
-    if (lane == 0) qi = atomicAdd(&a.ctr[0], 1ull);
-    qi = __shfl_sync(0xffffffffu, qi, 0);
-    if (qi >= a.count) break;
-    const uint64_t n = a.n[qi];
-    uint32_t p = 0;
-    if (n >= 4 && !(n & 1)) {
-      if (n == 4) p = 2;
-      else if (n < kSmallN) p = minp_plain(a, n);
-      else p = minp_big(a, n, buf);
+  // the lane's query
+  bool have = false, drained = false;
+  uint64_t qi = 0, n = 0;
+  uint32_t lim = 0, nm1 = 0, nm2 = 0, nm3 = 0;
+  uint32_t kb = 1;      // prime index of the next candidate batch
+  uint32_t cmask = 0;   // the current batch's survivors not yet tested
+  uint32_t cbase = 0;   // prime index of the current batch's bit 0
+  bool last = false;    // the current batch reached the end of the candidates
+  int stage = 0;        // 0: next candidate, base 2; k = 1..6: base k of the set
+  uint32_t p = 0;       // the candidate under test
+  bool ready = false;   // p taken for this round (stage 0)
+  Mont M{3, 0, 1};
+  uint64_t d = 1, r2 = 0;
+  int s = 1;
+  uint32_t found = 0, maxp = 0;
+  auto finish = [&](uint32_t pf) {
+    a.p_out[qi] = pf;
+    a.q_out[qi] = pf ? n - pf : 0;
+    if (pf) {
+      ++found;
+      maxp = pf > maxp ? pf : maxp;
     }
-    if (lane == 0) {
-      a.p_out[qi] = p;
-      a.q_out[qi] = p ? n - p : 0;
-      if (p) {
-        atomicAdd(&a.ctr[1], 1ull);
-        atomicMax(&a.ctr[2], (unsigned long long)p);
+    have = false;
+  };
+  for (;;) {
+    // every lane gets a query with a candidate ready, or the queue is empty
+    for (;;) {
+      const uint32_t need = __ballot_sync(kFull, !have && !drained);
+      if (need) {
+        unsigned long long base = 0;
+        if (lane == __ffs(need) - 1) base = atomicAdd(&a.ctr[0], (unsigned long long)__popc(need));
+        base = __shfl_sync(kFull, base, __ffs(need) - 1);
+        if (!have && !drained) {
+          qi = base + __popc(need & lanemask_lt());
+          if (qi >= a.count) {
+            drained = true;
+          } else {
+            n = a.n[qi];
+            have = true;
+            stage = 0;
+            kb = 1;
+            cmask = 0;
+            last = false;
+            const uint64_t half = n >> 1;
+            lim = (uint32_t)(half < a.p_lim ? half : a.p_lim);
+            nm1 = (uint32_t)(n % kM1);
+            nm2 = (uint32_t)(n % kM2);
+            nm3 = (uint32_t)(n % kM3);
+            if (n < 4 || (n & 1)) finish(0);
+            else if (n == 4) finish(2);
+          }
+        }
+      }
+      // candidate batches for the lanes that ran out, one query at a time
+      for (;;) {
+        const uint32_t m = __ballot_sync(kFull, have && stage == 0 && !ready && cmask == 0 && !last);
+        if (!m) break;
+        const int j = __ffs(m) - 1;
+        const uint64_t nj = __shfl_sync(kFull, n, j);
+        const uint32_t limj = __shfl_sync(kFull, lim, j);
+        if (nj < kSmallN) {
+          const uint32_t pj = minp_plain(a, nj, limj);
+          if (lane == j) finish(pj);
+          continue;
+        }
+        const uint32_t kj = __shfl_sync(kFull, kb, j);
+        const uint32_t m1 = __shfl_sync(kFull, nm1, j);
+        const uint32_t m2 = __shfl_sync(kFull, nm2, j);
+        const uint32_t m3 = __shfl_sync(kFull, nm3, j);
+        const uint64_t k = (uint64_t)kj + lane;
+        const uint32_t pk = k < a.nprimes ? a.primes[k] : 0xffffffffu;
+        const bool valid = k < a.nprimes && pk <= limj;
+        const uint32_t pass = __ballot_sync(kFull, valid && no_small_factor(m1, m2, m3, pk));
+        const uint32_t vb = __ballot_sync(kFull, valid);
+        if (lane == j) {
+          cmask = pass;
+          cbase = kj;
+          kb = kj + 32;
+          last = vb != kFull;
+        }
+      }
+      // set up this round's test
+      if (have && stage == 0 && !ready) {
+        if (cmask == 0) {
+          finish(0);  // every prime p <= min(n/2, p_lim) tried
+        } else {
+          const int bit = __ffs(cmask) - 1;
+          cmask &= cmask - 1;
+          p = a.primes[cbase + bit];
+          ready = true;
+        }
+      }
+      if (!__ballot_sync(kFull, !have && !drained)) break;
+    }
+    if (!__any_sync(kFull, have)) break;
+    // one strong test per lane: base 2 of a new candidate, or base `stage`
+    uint64_t am = 0;
+    bool skip = false;
+    if (have) {
+      if (stage == 0) {
+        const uint64_t q = n - p;
+        d = q - 1;
+        s = __ffsll((long long)d) - 1;
+        d >>= s;
+        M = mont_init(q);
+        am = mod_dbl(M.one, M.n);  // 2
+      } else {
+        uint64_t b = kMR7Bases[stage];
+        if (b >= M.n) b %= M.n;
+        skip = b == 0;
+        am = mont_mul(b, r2, M);
       }
     }
+    const bool ok = sprp_warp(M, am, d, s, have) || skip;
+    ready = false;
+    if (have) {
+      if (!ok) {
+        stage = 0;  // composite (a base-2 pseudoprime when stage > 0)
+      } else if (stage == 0) {
+        // R^2 mod q = 2^64 in Montgomery form: 2 squared six times
+        uint64_t t = mod_dbl(M.one, M.n);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) t = mont_mul(t, t, M);
+        r2 = t;
+        stage = 1;
+      } else if (++stage == 7) {
+        finish(p);
+      }
+    }
+  }
+  // the warp's counts, one atomic each
+  found = __reduce_add_sync(kFull, found);
+  maxp = __reduce_max_sync(kFull, maxp);
+  if (lane == 0) {
+    if (found) atomicAdd(&a.ctr[1], (unsigned long long)found);
+    if (maxp) atomicMax(&a.ctr[2], (unsigned long long)maxp);
   }
 }
 
