@@ -150,6 +150,55 @@ __device__ __forceinline__ uint64_t mont_mul(uint64_t a, uint64_t b, const Mont&
   return r;
 }
 
+// The same product on 32-bit limbs with explicit carry chains (operand
+// scanning: the 128-bit a*b, then one reduction step per limb with
+// m = t_i * (-n^-1 mod 2^32), then one conditional subtraction picked by
+// the borrow mask).  ninv0 is the low word of Mont::ninv.
+__device__ __forceinline__ uint64_t mont_mul32(uint64_t a, uint64_t b, uint64_t n, uint32_t ninv0) {
+  const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32);
+  const uint32_t b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+  const uint32_t n0 = (uint32_t)n, n1 = (uint32_t)(n >> 32);
+  uint32_t r0, r1;
+  asm("{\n\t"
+      ".reg .u32 t0, t1, t2, t3, t4, m, s0, s1, bw;\n\t"
+      "mul.lo.u32 t0, %2, %4;\n\t"
+      "mul.hi.u32 t1, %2, %4;\n\t"
+      "mad.lo.cc.u32 t1, %3, %4, t1;\n\t"
+      "madc.hi.u32 t2, %3, %4, 0;\n\t"
+      "mad.lo.cc.u32 t1, %2, %5, t1;\n\t"
+      "madc.hi.cc.u32 t2, %2, %5, t2;\n\t"
+      "addc.u32 t3, 0, 0;\n\t"
+      "mad.lo.cc.u32 t2, %3, %5, t2;\n\t"
+      "madc.hi.u32 t3, %3, %5, t3;\n\t"
+      "mul.lo.u32 m, t0, %8;\n\t"
+      "mad.lo.cc.u32 t0, m, %6, t0;\n\t"
+      "madc.hi.cc.u32 t1, m, %6, t1;\n\t"
+      "addc.cc.u32 t2, t2, 0;\n\t"
+      "addc.cc.u32 t3, t3, 0;\n\t"
+      "addc.u32 t4, 0, 0;\n\t"
+      "mad.lo.cc.u32 t1, m, %7, t1;\n\t"
+      "madc.hi.cc.u32 t2, m, %7, t2;\n\t"
+      "addc.cc.u32 t3, t3, 0;\n\t"
+      "addc.u32 t4, t4, 0;\n\t"
+      "mul.lo.u32 m, t1, %8;\n\t"
+      "mad.lo.cc.u32 t1, m, %6, t1;\n\t"
+      "madc.hi.cc.u32 t2, m, %6, t2;\n\t"
+      "addc.cc.u32 t3, t3, 0;\n\t"
+      "addc.u32 t4, t4, 0;\n\t"
+      "mad.lo.cc.u32 t2, m, %7, t2;\n\t"
+      "madc.hi.cc.u32 t3, m, %7, t3;\n\t"
+      "addc.u32 t4, t4, 0;\n\t"
+      "sub.cc.u32 s0, t2, %6;\n\t"
+      "subc.cc.u32 s1, t3, %7;\n\t"
+      "subc.u32 bw, t4, 0;\n\t"
+      "lop3.b32 %0, t2, s0, bw, 0xE4;\n\t"
+      "lop3.b32 %1, t3, s1, bw, 0xE4;\n\t"
+      "}"
+      : "=r"(r0), "=r"(r1)
+      : "r"(a0), "r"(a1), "r"(b0), "r"(b1), "r"(n0), "r"(n1), "r"(ninv0));
+  return ((uint64_t)r1 << 32) | r0;
+}
+
 __device__ __forceinline__ uint64_t mod_dbl(uint64_t a, uint64_t n) {
   uint64_t s = a + a;
   if (s < a || s >= n) s -= n;

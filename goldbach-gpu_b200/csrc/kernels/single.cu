@@ -91,29 +91,50 @@ __device__ __forceinline__ bool no_small_factor(uint32_t nm1, uint32_t nm2, uint
   return !f;
 }
 
+// Montgomery context for mont_mul32: the modulus, -n^-1 mod 2^32 and R mod n.
+struct Mont32 {
+  uint64_t n;
+  uint64_t one;
+  uint32_t ni;
+};
+
+// R mod n without a 64-bit division: 2^(k+1) - n for the top bit k of n,
+// then doubled up to 2^64 (no doubling for n >= 2^63).
+__device__ __forceinline__ Mont32 mont32_init(uint64_t n) {
+  Mont32 M;
+  M.n = n;
+  M.ni = 0u - inv32((uint32_t)n);
+  const int k = 63 - __clzll(n);
+  uint64_t x = k == 63 ? 0 - n : (2ull << k) - n;
+  for (int j = k + 1; j < 64; ++j) x = mod_dbl(x, n);
+  M.one = x;
+  return M;
+}
+
 // Strong probable-prime test of every lane's odd modulus M.n = d 2^s + 1 to
 // its base a1 (Montgomery form), the loop lengths set by the warp's longest
 // exponent and largest s (lanes with act false only run along).
-__device__ __forceinline__ bool sprp_warp(const Mont& M, uint64_t a1, uint64_t d, int s, bool act) {
-  const uint64_t a2 = mont_mul(a1, a1, M);
-  const uint64_t a3 = mont_mul(a2, a1, M);
+__device__ __forceinline__ bool sprp_warp(const Mont32& M, uint64_t a1, uint64_t d, int s, bool act) {
+  const uint32_t ni = M.ni;
+  const uint64_t a2 = mont_mul32(a1, a1, M.n, ni);
+  const uint64_t a3 = mont_mul32(a2, a1, M.n, ni);
   const int top = 63 - __clzll(d);  // d >= 1
   const int T = (int)__reduce_max_sync(kFull, act ? (uint32_t)top : 0u) | 1;  // odd
   // bit pairs (i+1, i) from i = T-1 down to 0; the first pair starts x
   uint32_t b = (uint32_t)(d >> (T - 1)) & 3u;
   uint64_t x = b == 0 ? M.one : b == 1 ? a1 : b == 2 ? a2 : a3;
   for (int i = T - 3; i >= 0; i -= 2) {
-    x = mont_mul(x, x, M);
-    x = mont_mul(x, x, M);
+    x = mont_mul32(x, x, M.n, ni);
+    x = mont_mul32(x, x, M.n, ni);
     b = (uint32_t)(d >> i) & 3u;
-    x = mont_mul(x, b == 0 ? M.one : b == 1 ? a1 : b == 2 ? a2 : a3, M);
+    x = mont_mul32(x, b == 0 ? M.one : b == 1 ? a1 : b == 2 ? a2 : a3, M.n, ni);
   }
   const uint64_t mone = M.n - M.one;
   bool ok = x == M.one || x == mone;
   bool done = ok;
   const int S = (int)__reduce_max_sync(kFull, act ? (uint32_t)s : 0u);
   for (int i = 1; i < S; ++i) {
-    x = mont_mul(x, x, M);
+    x = mont_mul32(x, x, M.n, ni);
     if (!done && i < s) {
       if (x == mone) ok = done = true;
       else if (x == M.one) done = true;
@@ -135,7 +156,7 @@ __global__ void __launch_bounds__(kSingleThreads) single_kernel(SingleArgs a) {
   int stage = 0;        // 0: next candidate, base 2; k = 1..6: base k of the set
   uint32_t p = 0;       // the candidate under test
   bool ready = false;   // p taken for this round (stage 0)
-  Mont M{3, 0, 1};
+  Mont32 M{3, 1, 1};
   uint64_t d = 1, r2 = 0;
   int s = 1;
   uint32_t found = 0, maxp = 0;
@@ -228,13 +249,13 @@ __global__ void __launch_bounds__(kSingleThreads) single_kernel(SingleArgs a) {
         d = q - 1;
         s = __ffsll((long long)d) - 1;
         d >>= s;
-        M = mont_init(q);
+        M = mont32_init(q);
         am = mod_dbl(M.one, M.n);  // 2
       } else {
         uint64_t b = kMR7Bases[stage];
         if (b >= M.n) b %= M.n;
         skip = b == 0;
-        am = mont_mul(b, r2, M);
+        am = mont_mul32(b, r2, M.n, M.ni);
       }
     }
     const bool ok = sprp_warp(M, am, d, s, have) || skip;
@@ -246,7 +267,7 @@ __global__ void __launch_bounds__(kSingleThreads) single_kernel(SingleArgs a) {
         // R^2 mod q = 2^64 in Montgomery form: 2 squared six times
         uint64_t t = mod_dbl(M.one, M.n);
 #pragma unroll
-        for (int i = 0; i < 6; ++i) t = mont_mul(t, t, M);
+        for (int i = 0; i < 6; ++i) t = mont_mul32(t, t, M.n, M.ni);
         r2 = t;
         stage = 1;
       } else if (++stage == 7) {
