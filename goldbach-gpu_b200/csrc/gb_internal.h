@@ -71,7 +71,7 @@ struct RangeArgs {
   int layout6;
   const uint32_t* wheel6;  // kWheel6Words
   const uint2* a15;
-  uint2* surv;             // survivor lists: 3 per CTA of surv_cap entries each
+  uint2* surv;             // survivor lists: 6 per CTA of surv_cap entries each
   uint32_t surv_cap;       // >= words of one class bitset
 };
 

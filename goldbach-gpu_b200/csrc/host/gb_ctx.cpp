@@ -434,10 +434,10 @@ gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint
   if (bps < 1) bps = 1;
   uint64_t grid = (uint64_t)c->sm_count * bps;
   if (a.total_items < grid) grid = std::max<uint64_t>(1, a.total_items);
-  if (a.layout6 && a.total_items) {  // survivor lists of the two-phase search
+  if (a.layout6 && a.total_items) {  // survivor lists of the levelled search
     a.surv_cap = a.nbw;
     void* p = nullptr;
-    if ((st = ws_scratch(c, w, (size_t)grid * 3 * a.surv_cap * sizeof(uint2), &p)) != GB_OK) return st;
+    if ((st = ws_scratch(c, w, (size_t)grid * 6 * a.surv_cap * sizeof(uint2), &p)) != GB_OK) return st;
     a.surv = (uint2*)p;
   }
   if (a.total_items) {
@@ -620,11 +620,11 @@ uint64_t gb_estimate_device_bytes(const gb_config* cfg) {
   const uint64_t np = pi_upper(want);
   // primes + reciprocals + class offsets, the build bitset and scan
   // blocks, wheels, counters, histogram, the Phase-2 queue, and the range
-  // search's survivor lists (2 CTAs on up to 160 SMs, 3 lists of up to
-  // 2^20/96 + 512 words)
+  // search's survivor lists (2 CTAs on up to 160 SMs, 2 sets of 3 lists of
+  // up to 2^20/96 + 512 words)
   return np * 20 + want / 16 + (want / 65536 + 1) * 4 + (kWheelWords + kWheel6Words) * 4 +
          kCtrCount * 8 + GB_HIST_BINS * 8 + (1ull << 20) * sizeof(QEntry) +
-         320ull * 3 * ((1u << 20) / 96 + 512) * 8;
+         320ull * 6 * ((1u << 20) / 96 + 512) * 8;
 }
 
 gb_status gb_create(int device, const gb_config* cfg, gb_ctx** out) {

@@ -105,13 +105,16 @@ __global__ void __launch_bounds__(kRange6Threads, kRange6Blocks) range6_kernel(c
   Ctx6& cx = g_cx6;
   uint32_t* pat6 = smem6_pat();
   for (uint32_t i = tid; i < kWheel6Words; i += kRange6Threads) pat6[i] = a.wheel6[i];
-  if (tid == 0) cx.nbw = a.nbw;
+  if (tid == 0) {
+    cx.nbw = a.nbw;
+    cx.surv = a.surv + (size_t)blockIdx.x * 6 * a.surv_cap;
+    cx.surv_cap = a.surv_cap;
+  }
   __syncthreads();
   load_tables6(s);
   uint32_t* Q1 = smem6_q(0);
   uint32_t* Q5 = smem6_q(1);
   uint32_t* HIST = smem6_hist();
-  uint2* surv = a.surv + (size_t)blockIdx.x * 3 * a.surv_cap;
 
   for (;;) {
     if (tid == 0) {
@@ -119,9 +122,10 @@ __global__ void __launch_bounds__(kRange6Threads, kRange6Blocks) range6_kernel(c
       cx.fb = 0;
       cx.maxp = 0;
       cx.psum = 0;
-      cx.next_task = 0;
-      cx.next_task2 = 0;
-      cx.scnt[0] = cx.scnt[1] = cx.scnt[2] = 0;
+      for (int l = 0; l < kLevels6; ++l) {
+        cx.next_task[l] = 0;
+        cx.scnt[l][0] = cx.scnt[l][1] = cx.scnt[l][2] = 0;
+      }
       cx.maxk = 0;
     }
     for (uint32_t i = tid; i < kSmemHistBins; i += kRange6Threads) HIST[i] = 0;
@@ -164,7 +168,7 @@ __global__ void __launch_bounds__(kRange6Threads, kRange6Blocks) range6_kernel(c
     // q <= n - 3: the chunk's last n bounds the sieve (A + 2 cnt could pass 2^64)
     sieve_window6<kRange6Threads>(Q1, Q5, a.nbw, nbits, G0, A + 2ull * (cnt - 1), pat6, s.primes,
                                  a.magic, a.a15, a.nsieve, a.kcoop);
-    search_chunk6<MINP, kRange6Threads>(s, surv, a.surv_cap);
+    search_chunk6<MINP, kRange6Threads>(s);
   }
 }
 

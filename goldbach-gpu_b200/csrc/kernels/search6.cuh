@@ -36,10 +36,22 @@ namespace gb {
 
 constexpr uint32_t kE6UBits = 15;
 constexpr uint32_t kLockSteps6 = 128; // lockstep entries of each class sequence
-// Phase A runs every task through the first kSurvSteps6 entries; the words
-// still holding an unresolved n (about 1 in 6 near 1e12) go to a per-class
-// survivor list, and phase B runs them, densely packed, through the rest.
-constexpr uint32_t kSurvSteps6 = 40;
+// The lockstep runs in levels: level 0 takes every word of the chunk through
+// the entries [0, 28); each later level takes the words still holding an
+// unresolved n (a per-class survivor list written by the level before it,
+// densely packed) through its own span, and the last level runs to the end
+// of the table.  A word costs the steps of the task it sits in (a task ends
+// when all its words are resolved), so re-packing the survivors keeps the
+// slow words together: near 1e12 the words alive after 28, 40 and 56
+// entries are about 45%, 17% and 3.7%, and the levels take about 0.76 of
+// the word-steps of a single split at 40 entries (measured: 1.50 against
+// 1.55 ms for 2^30 even n near 1e12; the barrier between levels and the
+// survivor traffic take the rest; 3, 5 and 7 levels measured 1.51, 1.50
+// and 1.56 ms).
+constexpr int kLevels6 = 4;
+__host__ __device__ constexpr uint32_t level6_start(int l) {
+  return l == 0 ? 0u : l == 1 ? 28u : l == 2 ? 40u : 56u;
+}
 constexpr int kWT6 = 7;                      // U words per lane per warp task
 constexpr uint32_t kTaskWords6 = 32 * kWT6;  // words per warp task
 
@@ -60,16 +72,29 @@ struct Ctx6 {
   // the chunk's accounting (zeroed before the sieve)
   uint32_t fb, maxp;        // from the per-n tails (the histogram gives the rest)
   unsigned long long psum;  // likewise
-  uint32_t next_task;       // the chunk's next phase-A warp task
-  uint32_t next_task2;      // the chunk's next phase-B warp task
-  uint32_t scnt[3];         // survivor words of each class
+  uint32_t next_task[kLevels6];   // the chunk's next warp task of each level
+  uint32_t scnt[kLevels6][3];     // survivor words pushed by each level, per class
   uint32_t maxk;            // 1 + largest prime index in the chunk's histogram
+  // the CTA's survivor lists (fixed for the kernel): set b, class ri at
+  // surv + (3b + ri) surv_cap; level l writes set l & 1
+  uint2* surv;
+  uint32_t surv_cap;
 };
+
+
 
 __shared__ Ctx6 g_cx6;
 // dynamic shared memory of range6_kernel:
 //   class wheel patterns | Q1 | Q5 (nbw words each) | HIST | E0 | E2 | E4
 extern __shared__ uint32_t g_smem6[];
+
+__device__ __forceinline__ uint2* surv6_list(int b, int ri) {
+  return g_cx6.surv + (size_t)(3 * b + ri) * g_cx6.surv_cap;
+}
+__device__ __forceinline__ uint32_t level6_end(int ri, int l) {
+  const uint32_t len = g_cx6.len[ri];
+  return l + 1 < kLevels6 ? min(len, level6_start(l + 1)) : len;
+}
 
 __device__ __forceinline__ uint32_t* smem6_pat() { return g_smem6; }
 __device__ __forceinline__ uint32_t* smem6_q(uint32_t cls5) {
@@ -150,8 +175,8 @@ __device__ __noinline__ void tail_one6(const SearchParams& s, int ri, uint32_t m
   }
 }
 
-// Word indices of a lane's U words: strided from a base word (phase A) or
-// listed (phase B).
+// Word indices of a lane's U words: strided from a base word (level 0) or
+// listed (later levels).
 struct WordsStrided {
   uint32_t base;
   __device__ __forceinline__ uint32_t operator[](int i) const { return base + 32 * i; }
@@ -219,26 +244,25 @@ __device__ __forceinline__ uint32_t step6(const SearchParams& s, uint32_t (&U)[W
   return cnt;
 }
 
-// One warp task of class ri (rho = 2 ri).  Phase A (PB false): words
+// One warp task of class ri (rho = 2 ri) at level L, through the entries
+// [level6_start(L), level6_end(ri, L)).  Level 0 (LISTED false): words
 // [task*kTaskWords6, +kTaskWords6) of the class, lane l owning words
-// task*kTaskWords6 + l + 32i, through the first kSurvSteps6 entries; words
-// still unresolved are appended to the class's survivor list surv (at most
-// one entry per word, so it cannot overflow).  Phase B: entries
-// [task*kTaskWords6, +kTaskWords6) of that list through the remaining
-// entries, the words' unresolved bits written back in place.  Lockstep over
-// the class sequence with one window-word cache keyed by (offset, class).
-// Not inlined: the task gets the whole register file of the thread (the
-// chunk loop around it keeps nothing live across the call), and it calls
-// nothing.
-template <bool MINP, bool PB>
-__device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_t task,
-                                          uint2* __restrict__ surv) {
+// task*kTaskWords6 + l + 32i; later levels: the entries [task*kTaskWords6,
+// +kTaskWords6) of the class's survivor list of level L - 1.  Every level
+// but the last appends the words still unresolved to the class's list of
+// level L (at most one entry per word, so it cannot overflow); the last
+// level writes their bits back in place.  Lockstep over the class
+// sequence with one window-word cache keyed by (offset, class).  Not
+// inlined: the task gets the whole register file of the thread (the chunk
+// loop around it keeps nothing live across the call), and it calls nothing.
+template <bool MINP, bool LISTED>
+__device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_t task, int L) {
   const Ctx6& cx = g_cx6;
   const int lane = threadIdx.x & 31;
   const uint64_t n0 = cx.n[ri];
   uint32_t U[kWT6];
-  typename std::conditional<PB, WordsListed<kWT6>, WordsStrided>::type W;
-  if constexpr (!PB) {
+  typename std::conditional<LISTED, WordsListed<kWT6>, WordsStrided>::type W;
+  if constexpr (!LISTED) {
     const uint32_t M = cx.M[ri];
     const uint32_t nuw = (M + 31) >> 5;
     W.base = task * kTaskWords6 + lane;
@@ -259,11 +283,12 @@ __device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_
       if (MINP) s.minp[cx.base_idx + ((n0 - cx.A) >> 1)] = ri == 2 ? 2 : 3;
     }
   } else {
-    const uint32_t cnt = cx.scnt[ri];
+    const uint2* in = surv6_list((L - 1) & 1, ri);
+    const uint32_t cnt_in = cx.scnt[L - 1][ri];
 #pragma unroll
     for (int i = 0; i < kWT6; ++i) {
       const uint32_t j = task * kTaskWords6 + lane + 32 * i;
-      const uint2 v = j < cnt ? surv[j] : make_uint2(0u, 0u);
+      const uint2 v = j < cnt_in ? in[j] : make_uint2(0u, 0u);
       W.w[i] = v.x;
       U[i] = v.y;
     }
@@ -272,12 +297,11 @@ __device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_
   const uint32_t* __restrict__ Q1 = smem6_q(0);
   const uint32_t* __restrict__ Q5 = smem6_q(1);
   uint32_t* HIST = smem6_hist();
-  const uint32_t len = cx.len[ri];
-  const uint32_t pos0 = PB ? kSurvSteps6 : 0;
-  const uint32_t pend = PB ? len : (len < kSurvSteps6 ? len : kSurvSteps6);
   const uint32_t K1 = cx.K[ri][0], K5 = cx.K[ri][1];
   const uint64_t ibase = cx.base_idx + ((n0 - cx.A) >> 1);
   Cache6<kWT6> ca;
+  const uint32_t pos0 = level6_start(L), pend = level6_end(ri, L);
+#pragma unroll 1
   for (uint32_t pos = pos0; pos < pend; ++pos) {
     if (((pos - pos0) & 7) == 0) {
       uint32_t any = 0;
@@ -295,75 +319,71 @@ __device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_
     cnt = __reduce_add_sync(0xffffffffu, cnt);
     if (lane == 0 && cnt) atomicAdd(&HIST[e6_k(e)], cnt);
   }
-  if constexpr (!PB) {
-    // unresolved words continue in phase B
+  if (L + 1 < kLevels6) {
+    uint2* out = surv6_list(L & 1, ri);
+    uint32_t* out_cnt = &g_cx6.scnt[L][ri];
     const uint32_t lt = (1u << lane) - 1;
 #pragma unroll
     for (int i = 0; i < kWT6; ++i) {
       const uint32_t alive = __ballot_sync(0xffffffffu, U[i] != 0);
       if (alive) {
         uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(&g_cx6.scnt[ri], (uint32_t)__popc(alive));
+        if (lane == 0) base = atomicAdd(out_cnt, (uint32_t)__popc(alive));
         base = __shfl_sync(0xffffffffu, base, 0);
-        if (U[i]) surv[base + __popc(alive & lt)] = make_uint2(W[i], U[i]);
+        if (U[i]) out[base + __popc(alive & lt)] = make_uint2(W[i], U[i]);
       }
     }
   } else {
-    // what is left goes back in place for the per-n pass
-    const uint32_t cnt = cx.scnt[ri];
+    uint2* in = surv6_list((L - 1) & 1, ri);
+    const uint32_t cnt_in = cx.scnt[L - 1][ri];
 #pragma unroll
     for (int i = 0; i < kWT6; ++i) {
       const uint32_t j = task * kTaskWords6 + lane + 32 * i;
-      if (j < cnt) surv[j].y = U[i];
+      if (j < cnt_in) in[j].y = U[i];
     }
   }
 }
 
 // Whole-chunk search by the CTA plus the flush of its accounting (same
 // contract as search_chunk in search.cuh).  The histogram, g_cx6's fb,
-// maxp, psum, maxk, scnt and task counters must be zero before the call.
-// Warps take tasks from shared counters, classes 2 and 4 first; surv holds
-// the CTA's three survivor lists of surv_cap entries (>= words of a class).
-// Ends with __syncthreads().
+// maxp, psum, maxk, scnt and next_task must be zero before the call, and
+// g_cx6's survivor lists set (surv_cap >= words of a class).  Warps take
+// each level's tasks from a shared counter, classes 2 and 4 first.  Ends
+// with __syncthreads().  (Two task call sites, the level a run-time
+// argument: one call site per level made ptxas spill in every task.)
 template <bool MINP, int NT>
-__device__ __forceinline__ void search_chunk6(const SearchParams& s, uint2* surv,
-                                              uint32_t surv_cap) {
+__device__ __forceinline__ void search_chunk6(const SearchParams& s) {
   const int tid = threadIdx.x;
   const int lane = tid & 31;
-  {
-    const uint32_t t0 = (((g_cx6.M[0] + 31) >> 5) + kTaskWords6 - 1) / kTaskWords6;
-    const uint32_t t2 = (((g_cx6.M[1] + 31) >> 5) + kTaskWords6 - 1) / kTaskWords6;
-    const uint32_t t4 = (((g_cx6.M[2] + 31) >> 5) + kTaskWords6 - 1) / kTaskWords6;
-    for (;;) {  // phase A
-      uint32_t task = 0;
-      if (lane == 0) task = atomicAdd(&g_cx6.next_task, 1u);
-      task = __shfl_sync(0xffffffffu, task, 0);
-      if (task >= t0 + t2 + t4) break;
-      const int ri = task < t2 ? 1 : task < t2 + t4 ? 2 : 0;
-      const uint32_t t = ri == 1 ? task : ri == 2 ? task - t2 : task - t2 - t4;
-      search_task6<MINP, false>(s, ri, t, surv + ri * surv_cap);
+#pragma unroll 1
+  for (int l = 0; l < kLevels6; ++l) {
+    uint32_t b0, b2, b4;
+    if (l == 0) {  // every word of the chunk
+      b0 = (((g_cx6.M[0] + 31) >> 5) + kTaskWords6 - 1) / kTaskWords6;
+      b2 = (((g_cx6.M[1] + 31) >> 5) + kTaskWords6 - 1) / kTaskWords6;
+      b4 = (((g_cx6.M[2] + 31) >> 5) + kTaskWords6 - 1) / kTaskWords6;
+    } else {  // the survivor lists of the level before
+      b0 = (g_cx6.scnt[l - 1][0] + kTaskWords6 - 1) / kTaskWords6;
+      b2 = (g_cx6.scnt[l - 1][1] + kTaskWords6 - 1) / kTaskWords6;
+      b4 = (g_cx6.scnt[l - 1][2] + kTaskWords6 - 1) / kTaskWords6;
     }
-  }
-  __syncthreads();
-  {
-    const uint32_t b0 = (g_cx6.scnt[0] + kTaskWords6 - 1) / kTaskWords6;
-    const uint32_t b2 = (g_cx6.scnt[1] + kTaskWords6 - 1) / kTaskWords6;
-    const uint32_t b4 = (g_cx6.scnt[2] + kTaskWords6 - 1) / kTaskWords6;
-    for (;;) {  // phase B
+    for (;;) {
       uint32_t task = 0;
-      if (lane == 0) task = atomicAdd(&g_cx6.next_task2, 1u);
+      if (lane == 0) task = atomicAdd(&g_cx6.next_task[l], 1u);
       task = __shfl_sync(0xffffffffu, task, 0);
       if (task >= b0 + b2 + b4) break;
       const int ri = task < b2 ? 1 : task < b2 + b4 ? 2 : 0;
       const uint32_t t = ri == 1 ? task : ri == 2 ? task - b2 : task - b2 - b4;
-      search_task6<MINP, true>(s, ri, t, surv + ri * surv_cap);
+      if (l == 0) search_task6<MINP, false>(s, ri, t, 0);
+      else search_task6<MINP, true>(s, ri, t, l);
     }
+    __syncthreads();
   }
-  __syncthreads();
-  // phase C: the n still unresolved after every lockstep entry, one per thread
+  // the n still unresolved after every lockstep entry, one per thread
   for (int ri = 0; ri < 3; ++ri) {
-    const uint2* L = surv + ri * surv_cap;
-    for (uint32_t j = tid; j < g_cx6.scnt[ri]; j += NT) {
+    const uint2* L = surv6_list((kLevels6 - 2) & 1, ri);
+    const uint32_t cnt = g_cx6.scnt[kLevels6 - 2][ri];
+    for (uint32_t j = tid; j < cnt; j += NT) {
       const uint2 v = L[j];
       uint32_t u = v.y;
       while (u) {

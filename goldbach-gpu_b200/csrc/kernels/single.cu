@@ -22,7 +22,9 @@
 //      by the two exponent bits) over the warp's longest exponent, so lanes
 //      with different q and bases never diverge.
 // Queries n < 2^21 (where q may be a prime <= 61) take a warp-cooperative
-// scan with the full test per candidate instead.
+// scan with the full test per candidate instead.  Small batches, where
+// latency rather than throughput sets the time, take single_warp_kernel
+// (one warp per query).
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -284,8 +286,118 @@ __global__ void __launch_bounds__(kSingleThreads) single_kernel(SingleArgs a) {
   }
 }
 
+// Latency path for small batches: one warp per query.  Survivors of the
+// small-prime filter are gathered in order (shared memory) until 32 are
+// pending; each lane runs the base-2 test on one of them, and the lowest
+// lane that passed gets the six other bases, one base per lane.  A lone
+// query then costs about two strong-test latencies instead of the dozen
+// the lane-per-query kernel spends on it one after another.
+__device__ uint32_t minp_warp(const SingleArgs& a, uint64_t n, uint32_t* buf) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t half = n >> 1;
+  const uint32_t lim = (uint32_t)(half < a.p_lim ? half : a.p_lim);
+  const uint32_t nm1 = (uint32_t)(n % kM1), nm2 = (uint32_t)(n % kM2), nm3 = (uint32_t)(n % kM3);
+  uint64_t k = 1;
+  uint32_t nsurv = 0;
+  bool exhausted = false;
+  for (;;) {
+    while (nsurv < 32 && !exhausted) {
+      const uint64_t kk = k + lane;
+      const uint32_t p = kk < a.nprimes ? a.primes[kk] : 0xffffffffu;
+      const bool valid = kk < a.nprimes && p <= lim;
+      const bool pass = valid && no_small_factor(nm1, nm2, nm3, p);
+      const uint32_t b = __ballot_sync(kFull, pass);
+      if (pass) buf[nsurv + __popc(b & lanemask_lt())] = (uint32_t)kk;
+      nsurv += __popc(b);
+      if (__ballot_sync(kFull, valid) != kFull) exhausted = true;
+      k += 32;
+    }
+    __syncwarp();
+    if (nsurv == 0) return 0;
+    const uint32_t take = nsurv < 32 ? nsurv : 32;
+    const bool act = lane < (int)take;
+    uint32_t pk = 0;
+    uint64_t q = 3;
+    if (act) {
+      pk = a.primes[buf[lane]];
+      q = n - pk;
+    }
+    uint64_t d = q - 1;
+    int s = __ffsll((long long)d) - 1;
+    d >>= s;
+    Mont32 M = mont32_init(q);
+    const bool ok2 = sprp_warp(M, mod_dbl(M.one, M.n), d, s, act) && act;
+    uint32_t b = __ballot_sync(kFull, ok2);
+    while (b) {
+      const int l = __ffs(b) - 1;
+      const uint64_t qc = __shfl_sync(kFull, q, l);
+      const uint32_t pc = __shfl_sync(kFull, pk, l);
+      uint64_t dc = qc - 1;
+      const int sc = __ffsll((long long)dc) - 1;
+      dc >>= sc;
+      const Mont32 Mc = mont32_init(qc);
+      uint64_t r2 = mod_dbl(Mc.one, Mc.n);
+#pragma unroll
+      for (int i = 0; i < 6; ++i) r2 = mont_mul32(r2, r2, Mc.n, Mc.ni);
+      uint64_t base = kMR7Bases[lane < 6 ? lane + 1 : 1];
+      if (base >= qc) base %= qc;
+      const bool test = lane < 6 && base != 0;
+      const bool ok = sprp_warp(Mc, mont_mul32(base, r2, Mc.n, Mc.ni), dc, sc, test) || !test;
+      if (__all_sync(kFull, ok)) return pc;
+      b &= b - 1;
+    }
+    // none of the first `take` survivors is prime: drop them
+    __syncwarp();
+    uint32_t keep = 0;
+    if (lane + take < nsurv) keep = buf[lane + take];
+    __syncwarp();
+    if (lane + take < nsurv) buf[lane] = keep;
+    __syncwarp();
+    nsurv -= take;
+  }
+}
+
+__global__ void __launch_bounds__(kSingleThreads) single_warp_kernel(SingleArgs a) {
+  __shared__ uint32_t sbuf[kSingleThreads / 32][64];
+  const int lane = threadIdx.x & 31;
+  uint32_t* buf = sbuf[threadIdx.x >> 5];
+  uint32_t found = 0, maxp = 0;
+  for (;;) {
+    unsigned long long qi = 0;
+    if (lane == 0) qi = atomicAdd(&a.ctr[0], 1ull);
+    qi = __shfl_sync(kFull, qi, 0);
+    if (qi >= a.count) break;
+    const uint64_t n = a.n[qi];
+    uint32_t p = 0;
+    if (n >= 4 && !(n & 1)) {
+      const uint64_t half = n >> 1;
+      if (n == 4) p = 2;
+      else if (n < kSmallN) p = minp_plain(a, n, half < a.p_lim ? half : a.p_lim);
+      else p = minp_warp(a, n, buf);
+    }
+    if (lane == 0) {
+      a.p_out[qi] = p;
+      a.q_out[qi] = p ? n - p : 0;
+      if (p) {
+        ++found;
+        maxp = p > maxp ? p : maxp;
+      }
+    }
+  }
+  if (lane == 0) {
+    if (found) atomicAdd(&a.ctr[1], (unsigned long long)found);
+    if (maxp) atomicMax(&a.ctr[2], (unsigned long long)maxp);
+  }
+}
+
+// Batches below kLaneBatchMin queries take the warp-per-query kernel: they
+// fit the GPU's resident warps at once, so the per-query latency (about
+// two strong tests there, a dozen per lane in single_kernel) sets the time.
+constexpr uint64_t kLaneBatchMin = 8192;
+
 cudaError_t launch_single(const SingleArgs& a, int grid, cudaStream_t s) {
-  single_kernel<<<grid, kSingleThreads, 0, s>>>(a);
+  if (a.count < kLaneBatchMin) single_warp_kernel<<<grid, kSingleThreads, 0, s>>>(a);
+  else single_kernel<<<grid, kSingleThreads, 0, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -53,3 +53,19 @@ def test_agrees_with_range_path(ctx):
     n = start + 2 * np.arange(4096, dtype=np.uint64)
     p, _, _ = ctx.check_single(n)
     np.testing.assert_array_equal(p, r.min_p.astype(np.uint64))
+
+
+def test_small_and_large_batches_agree(ctx, oracle):
+    """Batches below 8192 queries take the warp-per-query kernel, larger ones
+    the lane-per-query kernel: the same n give the same (p, q) either way."""
+    rng = np.random.default_rng(11)
+    n = (rng.integers(2, 2**63, size=12000, dtype=np.uint64) * 2).astype(np.uint64)
+    n[:40] = np.arange(4, 84, 2, dtype=np.uint64)  # the plain path for small n too
+    p_big, q_big, r = ctx.check_single(n)
+    parts = [ctx.check_single(n[i:i + 1000]) for i in range(0, len(n), 1000)]
+    p_small = np.concatenate([x[0] for x in parts])
+    q_small = np.concatenate([x[1] for x in parts])
+    np.testing.assert_array_equal(p_big, p_small)
+    np.testing.assert_array_equal(q_big, q_small)
+    np.testing.assert_array_equal(p_big, oracle.single_minp(n))
+    assert r.found == len(n) and sum(x[2].found for x in parts) == len(n)
