@@ -287,7 +287,9 @@ def measure_counts(gb, ctx, points=((10**9, 4096), (10**10, 1024))):
 def measure_serving(gb, device, rates=(1e2, 1e3, 1e4, 1e5), seconds=2.0, max_requests=10000):
     """C5: Poisson arrivals (seed 3) per rate; 70% single n uniform in
     [4, 2^64-2], 30% ranges of log-uniform width 2^8..2^26 even n at
-    offsets uniform in [4, 1e19]; latency from scheduled arrival."""
+    offsets uniform in [4, 1e19]; latency from scheduled arrival.  The
+    load generator polls the clock for the last 200 us before each arrival
+    (a sleep there would submit late by the timer slack, ~50-100 us)."""
     import numpy as np
     out = []
     with gb.Context(device) as ctx:
@@ -315,8 +317,10 @@ def measure_serving(gb, device, rates=(1e2, 1e3, 1e4, 1e5), seconds=2.0, max_req
                 if j > i:
                     tickets += list(ctx.submit(kinds[i:j], a[i:j], cnt[i:j], arr[i:j]))
                     i = j
-                else:
-                    time.sleep(min(0.0005, max(0.0, (int(arr[i]) - now) / 1e9)))
+                else:  # sleep until 200 us before the next arrival, then poll
+                    ahead = (int(arr[i]) - now) / 1e9
+                    if ahead > 300e-6:
+                        time.sleep(min(0.0005, ahead - 200e-6))
             res = [ctx.wait(t, 600000) for t in tickets]
             st = ctx.serve_stats()
             lat_s = np.array([r["latency_us"] for r, k in zip(res, kinds) if k == 0 and r["status"] == 0])

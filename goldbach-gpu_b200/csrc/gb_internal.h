@@ -160,7 +160,22 @@ struct SingleArgs {
   uint64_t p_lim;
   unsigned long long* ctr;  // [0] work, [1] found, [2] max p
 };
+// Batches below kLaneBatchMin queries take the warp-per-query kernel (latency),
+// larger ones the lane-per-query kernel (throughput).
+constexpr uint64_t kLaneBatchMin = 8192;
 cudaError_t launch_single(const SingleArgs& a, int grid, cudaStream_t s);
+// Arguments of segment_reduce_kernel, kept together for a graph's kernel node.
+struct SegReduceArgs {
+  const uint64_t* p;
+  const uint64_t* off;
+  uint32_t nreq;
+  unsigned long long* agg;
+};
+// Kernel-node parameters of the launches launch_single / launch_segment_reduce
+// would make (argv: caller storage for the argument pointers; a, r and argv
+// must stay alive until the node is added or updated).
+void single_kernel_node(const SingleArgs& a, int grid, void** argv, cudaKernelNodeParams* kp);
+void segment_reduce_node(const SegReduceArgs& r, void** argv, cudaKernelNodeParams* kp);
 cudaError_t launch_is_prime(const uint64_t* n, uint64_t count, uint8_t* out, cudaStream_t s);
 cudaError_t launch_win_expand(const gb_window* w, const uint64_t* off, uint32_t nw, uint64_t* n,
                               cudaStream_t s);

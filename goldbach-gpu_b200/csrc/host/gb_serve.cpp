@@ -64,6 +64,7 @@ struct gb_server {
   // single-lane pinned staging
   uint64_t *h_n = nullptr, *h_p = nullptr, *h_off = nullptr;
   unsigned long long* h_agg = nullptr;
+  bool single_graph = false;  // the single lane runs its small batches as a graph
   // stats
   std::vector<double> lat;
   uint64_t submitted = 0, completed = 0, rejected = 0, t0 = 0;
@@ -87,6 +88,92 @@ void finish(gb_server* S, const Pending& p, gb_response& resp, uint64_t t_done) 
   S->cv_done.notify_all();
 }
 
+// The single lane's batch pipeline (two uploads, the counter reset, the
+// single-n kernel, the per-request reduction, two downloads) as one CUDA
+// graph, built once with the lane's fixed buffers; each batch updates the
+// copy sizes and the two kernels' arguments and launches it.  Only batches
+// of fewer than kLaneBatchMin n use it (the kernel node is the
+// warp-per-query kernel).
+struct SingleGraph {
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t x = nullptr;
+  cudaGraphNode_t up_n = nullptr, up_off = nullptr, reset = nullptr, ks = nullptr,
+                  kr = nullptr, down_p = nullptr, down_agg = nullptr;
+  ~SingleGraph() {
+    if (x) cudaGraphExecDestroy(x);
+    if (g) cudaGraphDestroy(g);
+  }
+};
+
+struct SingleBufs {
+  uint64_t *d_n, *d_p, *d_q, *d_off;
+  unsigned long long* d_agg;
+};
+
+bool build_single_graph(gb_server* S, const SingleBufs& B, const SingleArgs& a0,
+                        SingleGraph* G) {
+  Lane& L = S->lane[0];
+  if (cudaGraphCreate(&G->g, 0) != cudaSuccess) return false;
+  // a chain: each node depends on the one before
+  bool ok = cudaGraphAddMemcpyNode1D(&G->up_n, G->g, nullptr, 0, B.d_n, S->h_n, 8,
+                                     cudaMemcpyHostToDevice) == cudaSuccess;
+  cudaGraphNode_t prev = G->up_n;
+  ok = ok && cudaGraphAddMemcpyNode1D(&G->up_off, G->g, &prev, 1, B.d_off, S->h_off, 16,
+                                      cudaMemcpyHostToDevice) == cudaSuccess;
+  prev = G->up_off;
+  cudaMemsetParams ms{};
+  ms.dst = L.ws.ctr;
+  ms.value = 0;
+  ms.elementSize = 4;
+  ms.width = 8;  // 4 counters of 8 bytes
+  ms.height = 1;
+  ok = ok && cudaGraphAddMemsetNode(&G->reset, G->g, &prev, 1, &ms) == cudaSuccess;
+  prev = G->reset;
+  void* argv[4];
+  cudaKernelNodeParams kp;
+  single_kernel_node(a0, 1, argv, &kp);
+  ok = ok && cudaGraphAddKernelNode(&G->ks, G->g, &prev, 1, &kp) == cudaSuccess;
+  prev = G->ks;
+  const SegReduceArgs r0{B.d_p, B.d_off, 1, B.d_agg};
+  segment_reduce_node(r0, argv, &kp);
+  ok = ok && cudaGraphAddKernelNode(&G->kr, G->g, &prev, 1, &kp) == cudaSuccess;
+  prev = G->kr;
+  ok = ok && cudaGraphAddMemcpyNode1D(&G->down_p, G->g, &prev, 1, S->h_p, B.d_p, 8,
+                                      cudaMemcpyDeviceToHost) == cudaSuccess;
+  prev = G->down_p;
+  ok = ok && cudaGraphAddMemcpyNode1D(&G->down_agg, G->g, &prev, 1, S->h_agg, B.d_agg, 32,
+                                      cudaMemcpyDeviceToHost) == cudaSuccess;
+  ok = ok && cudaGraphInstantiate(&G->x, G->g, 0) == cudaSuccess;
+  if (!ok) cudaGetLastError();
+  return ok;
+}
+
+// One batch through the graph: pos n, nreq requests, args a (count = pos).
+cudaError_t run_single_graph(gb_server* S, const SingleBufs& B, const SingleArgs& a, int grid,
+                             uint32_t nreq, SingleGraph* G) {
+  Lane& L = S->lane[0];
+  const uint64_t pos = a.count;
+  cudaError_t e;
+  if ((e = cudaGraphExecMemcpyNodeSetParams1D(G->x, G->up_n, B.d_n, S->h_n, pos * 8,
+                                              cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaGraphExecMemcpyNodeSetParams1D(G->x, G->up_off, B.d_off, S->h_off,
+                                              (nreq + 1) * 8ull, cudaMemcpyHostToDevice)) !=
+          cudaSuccess ||
+      (e = cudaGraphExecMemcpyNodeSetParams1D(G->x, G->down_p, S->h_p, B.d_p, pos * 8,
+                                              cudaMemcpyDeviceToHost)) != cudaSuccess ||
+      (e = cudaGraphExecMemcpyNodeSetParams1D(G->x, G->down_agg, S->h_agg, B.d_agg, nreq * 32ull,
+                                              cudaMemcpyDeviceToHost)) != cudaSuccess)
+    return e;
+  void* argv[4];
+  cudaKernelNodeParams kp;
+  single_kernel_node(a, grid, argv, &kp);
+  if ((e = cudaGraphExecKernelNodeSetParams(G->x, G->ks, &kp)) != cudaSuccess) return e;
+  const SegReduceArgs r{B.d_p, B.d_off, nreq, B.d_agg};
+  segment_reduce_node(r, argv, &kp);
+  if ((e = cudaGraphExecKernelNodeSetParams(G->x, G->kr, &kp)) != cudaSuccess) return e;
+  return cudaGraphLaunch(G->x, L.stream);
+}
+
 void single_lane(gb_server* S) {
   Lane& L = S->lane[0];
   gb_ctx* c = S->c;
@@ -99,6 +186,19 @@ void single_lane(gb_server* S) {
   unsigned long long* d_agg = (unsigned long long*)L.arena.take((size_t)kSingleReqCap * 32);
   uint64_t np = 0;
   count_le(c, L.ws, GB_PHASE2_LIMIT_DEFAULT, &np);
+  const SingleBufs B{d_n, d_p, d_q, d_off, d_agg};
+  SingleArgs base{};
+  base.n = d_n;
+  base.count = 1;
+  base.p_out = d_p;
+  base.q_out = d_q;
+  base.primes = c->d_primes;
+  base.nprimes = np;
+  base.p_lim = GB_PHASE2_LIMIT_DEFAULT;
+  base.ctr = L.ws.ctr;
+  SingleGraph G;
+  const bool graph = !S->o.no_graph && build_single_graph(S, B, base, &G);
+  S->single_graph = graph;
   std::vector<Pending> take;
   for (;;) {
     take.clear();
@@ -129,23 +229,20 @@ void single_lane(gb_server* S) {
     auto chk = [&](cudaError_t x) {
       if (e == cudaSuccess && x != cudaSuccess) e = x;
     };
-    chk(cudaMemcpyAsync(d_n, S->h_n, pos * 8, cudaMemcpyHostToDevice, L.stream));
-    chk(cudaMemcpyAsync(d_off, S->h_off, (take.size() + 1) * 8, cudaMemcpyHostToDevice, L.stream));
-    chk(cudaMemsetAsync(L.ws.ctr, 0, 4 * 8, L.stream));
-    SingleArgs a{};
-    a.n = d_n;
+    SingleArgs a = base;
     a.count = pos;
-    a.p_out = d_p;
-    a.q_out = d_q;
-    a.primes = c->d_primes;
-    a.nprimes = np;
-    a.p_lim = GB_PHASE2_LIMIT_DEFAULT;
-    a.ctr = L.ws.ctr;
     const uint64_t grid = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)c->sm_count * 6, (pos + 7) / 8));
-    chk(launch_single(a, (int)grid, L.stream));
-    chk(launch_segment_reduce(d_p, d_off, (uint32_t)take.size(), d_agg, L.stream));
-    chk(cudaMemcpyAsync(S->h_p, d_p, pos * 8, cudaMemcpyDeviceToHost, L.stream));
-    chk(cudaMemcpyAsync(S->h_agg, d_agg, take.size() * 32, cudaMemcpyDeviceToHost, L.stream));
+    if (graph && pos < kLaneBatchMin) {
+      chk(run_single_graph(S, B, a, (int)grid, (uint32_t)take.size(), &G));
+    } else {
+      chk(cudaMemcpyAsync(d_n, S->h_n, pos * 8, cudaMemcpyHostToDevice, L.stream));
+      chk(cudaMemcpyAsync(d_off, S->h_off, (take.size() + 1) * 8, cudaMemcpyHostToDevice, L.stream));
+      chk(cudaMemsetAsync(L.ws.ctr, 0, 4 * 8, L.stream));
+      chk(launch_single(a, (int)grid, L.stream));
+      chk(launch_segment_reduce(d_p, d_off, (uint32_t)take.size(), d_agg, L.stream));
+      chk(cudaMemcpyAsync(S->h_p, d_p, pos * 8, cudaMemcpyDeviceToHost, L.stream));
+      chk(cudaMemcpyAsync(S->h_agg, d_agg, take.size() * 32, cudaMemcpyDeviceToHost, L.stream));
+    }
     chk(cudaStreamSynchronize(L.stream));
     const uint64_t t_done = now_ns();
     const uint32_t batch = (uint32_t)L.batches++;

@@ -393,12 +393,19 @@ __global__ void __launch_bounds__(kSingleThreads) single_warp_kernel(SingleArgs 
 // Batches below kLaneBatchMin queries take the warp-per-query kernel: they
 // fit the GPU's resident warps at once, so the per-query latency (about
 // two strong tests there, a dozen per lane in single_kernel) sets the time.
-constexpr uint64_t kLaneBatchMin = 8192;
-
 cudaError_t launch_single(const SingleArgs& a, int grid, cudaStream_t s) {
   if (a.count < kLaneBatchMin) single_warp_kernel<<<grid, kSingleThreads, 0, s>>>(a);
   else single_kernel<<<grid, kSingleThreads, 0, s>>>(a);
   return cudaGetLastError();
+}
+
+void single_kernel_node(const SingleArgs& a, int grid, void** argv, cudaKernelNodeParams* kp) {
+  argv[0] = (void*)&a;
+  *kp = cudaKernelNodeParams{};
+  kp->func = a.count < kLaneBatchMin ? (void*)single_warp_kernel : (void*)single_kernel;
+  kp->gridDim = dim3((unsigned)grid);
+  kp->blockDim = dim3(kSingleThreads);
+  kp->kernelParams = argv;
 }
 
 // Per-request totals of a single-lane batch: request r owns the n of
@@ -439,6 +446,18 @@ cudaError_t launch_segment_reduce(const uint64_t* p, const uint64_t* off, uint32
   if (!nreq) return cudaSuccess;
   segment_reduce_kernel<<<(nreq + 7) / 8, 256, 0, s>>>(p, off, nreq, agg);
   return cudaGetLastError();
+}
+
+void segment_reduce_node(const SegReduceArgs& r, void** argv, cudaKernelNodeParams* kp) {
+  argv[0] = (void*)&r.p;
+  argv[1] = (void*)&r.off;
+  argv[2] = (void*)&r.nreq;
+  argv[3] = (void*)&r.agg;
+  *kp = cudaKernelNodeParams{};
+  kp->func = (void*)segment_reduce_kernel;
+  kp->gridDim = dim3((r.nreq + 7) / 8);
+  kp->blockDim = dim3(256);
+  kp->kernelParams = argv;
 }
 
 __global__ void is_prime_kernel(const uint64_t* n, uint64_t count, uint8_t* out) {

@@ -341,6 +341,9 @@ typedef struct gb_serve_opts {
   uint32_t max_range_batch;    /* requests per range-lane batch (0: 4096)      */
   uint64_t range_arena_bytes;  /* range-lane device memory (0: 4 GiB)          */
   uint64_t small_range;        /* ranges of <= this many n run n by n (0: 2^15) */
+  uint32_t no_graph;           /* 1: single-lane batches of < 8192 n as plain
+                                  stream launches instead of one CUDA graph   */
+  uint32_t reserved;           /* 0                                            */
 } gb_serve_opts;
 
 typedef struct gb_serve_stats {
