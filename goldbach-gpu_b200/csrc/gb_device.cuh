@@ -107,6 +107,20 @@ __device__ __forceinline__ uint32_t mod_p(uint64_t x, uint32_t p, uint64_t magic
   return (uint32_t)(r >= p ? r - p : r);
 }
 
+// The same remainder from a double-precision quotient estimate, inv the
+// correctly rounded 1/p.  The conversion of x, inv and the product each
+// carry a relative error of at most 2^-53, so the estimate is within
+// 3 * 2^-53 * x/p < 1 of x / p whenever x / p < 2^51 (every x < 2^64 for
+// p >= 2^13), its truncation is floor(x / p) - 1, + 0 or + 1, and one signed
+// correction of the 64-bit remainder x - q p (in (-p, 2p)) finishes it.
+__device__ __forceinline__ uint32_t mod_p_f64(uint64_t x, uint32_t p, double inv) {
+  const uint64_t q = (uint64_t)(__ull2double_rn(x) * inv);
+  int64_t r = (int64_t)(x - q * (uint64_t)p);
+  if (r < 0) r += p;
+  else if (r >= (int64_t)p) r -= p;
+  return (uint32_t)r;
+}
+
 // ---------------------------------------------------------------------------
 // Montgomery arithmetic modulo an odd 64-bit n, R = 2^64.
 struct Mont {

@@ -34,6 +34,18 @@ __device__ __forceinline__ uint64_t first_mark(int64_t g0, uint32_t p, uint64_t 
   return delta >> 1;
 }
 
+// first_mark with the remainder from a double-precision quotient estimate
+// (inv = 1/p correctly rounded; p >= 2^13) and gpp = (p^2 - 1) / 2 given.
+__device__ __forceinline__ uint64_t first_mark_f64(int64_t g0, uint32_t p, double inv,
+                                                   uint64_t gpp) {
+  if (g0 < 0 || (uint64_t)g0 <= gpp) return gpp - (uint64_t)g0;  // start at p^2
+  const uint64_t q0 = 2 * (uint64_t)g0 + 1;
+  const uint32_t r = mod_p_f64(q0, p, inv);
+  uint64_t delta = r ? p - r : 0;  // q0 + delta: the first multiple >= q0
+  if (delta & 1) delta += p;       // q0 is odd: the multiple is odd iff delta is even
+  return delta >> 1;
+}
+
 // Sieves bits [0, nbits) of the window into Q (nwords words are written;
 // nwords*32 >= nbits).  Bit i <-> q = 2*(g0 + i) + 1; set iff q is prime,
 // exact for every q <= q_top (q_top <= 2*(g0+nbits)-1).  `pat` is the

@@ -11,8 +11,10 @@
 //      and stored with coalesced stores;
 //   B. large primes: one thread per prime p in [2^17, sqrt(max q)] walks the
 //      windows (sorted by their top q, so only those with p^2 <= top are
-//      visited), computes the first multiple by Barrett reduction and clears
-//      its multiples with global atomicAnd (at most a few per window);
+//      visited), computes the first multiple from a double-precision
+//      quotient estimate (one remainder per window: the stage's whole cost)
+//      and clears its multiples with global atomicAnd (at most a few per
+//      window);
 //   C. search: every chunk of NE even n loads its q-window from HBM into
 //      shared memory and runs the same word-parallel search as the range
 //      kernel (search.cuh);
@@ -112,8 +114,9 @@ __global__ void __launch_bounds__(256) win_large_kernel(const __grid_constant__ 
   for (uint64_t k = a.nsmall + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < a.nlarge;
        k += stride) {
     const uint32_t p = a.s.primes[k];
-    const uint64_t magic = a.magic[k];
+    const double inv = 1.0 / (double)p;  // p >= 2^17: first_mark_f64 applies
     const uint64_t pp = (uint64_t)p * p;
+    const uint64_t gpp = (pp - 1) >> 1;
     uint32_t w0, w1;
     if (w_only < a.nwin) {
       w0 = w_only;
@@ -133,7 +136,7 @@ __global__ void __launch_bounds__(256) win_large_kernel(const __grid_constant__ 
     for (uint32_t w = w0; w < w1; ++w) {
       const WinDesc d = a.win[w];
       const int64_t g0 = (int64_t)(d.start >> 1) - (int64_t)(a.s.halo >> 1);
-      const uint64_t f = first_mark(g0, p, magic);
+      const uint64_t f = first_mark_f64(g0, p, inv, gpp);
       uint32_t* bw = a.bits + d.wbase;
       for (uint64_t i = f; i < d.wbits; i += p) atomicAnd(&bw[i >> 5], ~(1u << (i & 31)));
     }
