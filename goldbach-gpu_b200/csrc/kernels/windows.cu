@@ -8,7 +8,7 @@
 // staged through HBM:
 //   A. tile sieve: every window's odd q-bitset [start-H+1, end] is sieved
 //      tile by tile in shared memory with the wheel and the primes < 2^17,
-//      and stored with coalesced stores;
+//      and stored with coalesced 128-bit stores;
 //   B. large primes: one thread per prime p in [2^17, sqrt(max q)] walks the
 //      windows (sorted by their top q, so only those with p^2 <= top are
 //      visited), computes the first multiple from a double-precision
@@ -101,8 +101,10 @@ __global__ void __launch_bounds__(kWinThreads) win_tile_kernel(const __grid_cons
     const uint64_t q_top = gt >= (d.q_top >> 1) ? d.q_top : 2 * gt + 1;
     const uint32_t ns = d.nsieve < a.nsmall ? d.nsieve : a.nsmall;
     sieve_window<kWinThreads>(Q, nw, nb, g0, q_top, pat, a.s.primes, a.magic, ns, a.kcoop);
-    uint32_t* out = a.bits + d.wbase + b0 / 32;
-    for (uint32_t i = threadIdx.x; i < nw; i += kWinThreads) out[i] = Q[i];
+    // 128-bit coalesced stores: wbase, b0 / 32 and nw are multiples of 4 words
+    uint4* out = reinterpret_cast<uint4*>(a.bits + d.wbase + b0 / 32);
+    for (uint32_t i = threadIdx.x; i < nw / 4; i += kWinThreads)
+      out[i] = make_uint4(Q[4 * i], Q[4 * i + 1], Q[4 * i + 2], Q[4 * i + 3]);
     __syncthreads();
   }
 }
