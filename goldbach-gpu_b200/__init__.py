@@ -116,7 +116,7 @@ class Response(C.Structure):
 class ServeOpts(C.Structure):
     _fields_ = [("max_n", u64), ("max_single_batch", u32), ("max_range_batch", u32),
                 ("range_arena_bytes", u64), ("small_range", u64), ("no_graph", u32),
-                ("reserved", u32)]
+                ("spin_us", u32)]
 
 
 class ServeStats(C.Structure):
@@ -369,9 +369,10 @@ class Context:
 
     # -- serving ---------------------------------------------------------------
     def serve_start(self, max_n: int = 0, max_single_batch: int = 0, max_range_batch: int = 0,
-                    range_arena_bytes: int = 0, small_range: int = 0, no_graph: bool = False):
+                    range_arena_bytes: int = 0, small_range: int = 0, no_graph: bool = False,
+                    spin_us: int = 0):
         o = ServeOpts(max_n, max_single_batch, max_range_batch, range_arena_bytes, small_range,
-                      1 if no_graph else 0, 0)
+                      1 if no_graph else 0, spin_us)
         self._check(self.L.gb_serve_start(self._h, C.byref(o)))
 
     def submit(self, kinds, a, counts=None, arrival_ns=None) -> np.ndarray:

@@ -14,6 +14,7 @@
 // order, up to its batch size and arena), so requests that arrive while the
 // GPU is busy are admitted as soon as a lane and memory free up.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -57,6 +58,10 @@ struct gb_server {
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<Pending> q[2];
+  // requests queued per lane and the stop request, readable without the
+  // mutex by a lane that polls (opts.spin_us)
+  std::atomic<uint64_t> queued[2];
+  std::atomic<bool> stopping{false};
   std::unordered_map<uint64_t, gb_response> done;
   uint64_t next_ticket = 1;
   bool stop = false;
@@ -86,6 +91,16 @@ void finish(gb_server* S, const Pending& p, gb_response& resp, uint64_t t_done) 
   S->completed++;
   if (resp.status == GB_OK) S->lat.push_back(resp.latency_us);
   S->cv_done.notify_all();
+}
+
+// With opts.spin_us, a lane about to wait for work polls its queue for up to
+// that long first (a blocked thread takes tens of microseconds to wake).
+void poll_queue(gb_server* S, int ln) {
+  if (!S->o.spin_us) return;
+  const uint64_t end = now_ns() + 1000ull * S->o.spin_us;
+  while (!S->queued[ln].load(std::memory_order_acquire) &&
+         !S->stopping.load(std::memory_order_relaxed) && now_ns() < end)
+    std::this_thread::yield();
 }
 
 // The single lane's batch pipeline (two uploads, the counter reset, the
@@ -205,6 +220,9 @@ void single_lane(gb_server* S) {
     uint64_t total = 0;
     {
       std::unique_lock<std::mutex> lk(S->mu);
+      lk.unlock();
+      poll_queue(S, 0);
+      lk.lock();
       S->cv_work.wait(lk, [&] { return S->stop || !S->q[0].empty(); });
       if (S->q[0].empty()) break;  // stop requested and drained
       while (!S->q[0].empty() && take.size() < kSingleReqCap) {
@@ -214,6 +232,7 @@ void single_lane(gb_server* S) {
         take.push_back(f);
         total += w;
         S->q[0].pop_front();
+        S->queued[0].fetch_sub(1, std::memory_order_relaxed);
       }
     }
     uint64_t pos = 0;
@@ -277,6 +296,9 @@ void range_lane(gb_server* S) {
     take.clear();
     {
       std::unique_lock<std::mutex> lk(S->mu);
+      lk.unlock();
+      poll_queue(S, 1);
+      lk.lock();
       S->cv_work.wait(lk, [&] { return S->stop || !S->q[1].empty(); });
       if (S->q[1].empty()) break;
       uint64_t bytes = 64 << 10;
@@ -287,6 +309,7 @@ void range_lane(gb_server* S) {
         take.push_back(f);
         bytes += b;
         S->q[1].pop_front();
+        S->queued[1].fetch_sub(1, std::memory_order_relaxed);
       }
     }
     win.resize(take.size());
@@ -348,6 +371,8 @@ gb_status gb_serve_start(gb_ctx* c, const gb_serve_opts* opts) {
   if (c->server) return GB_EINVAL;
   cudaSetDevice(c->device);
   gb_server* S = new gb_server();
+  S->queued[0] = 0;
+  S->queued[1] = 0;
   S->c = c;
   if (opts) S->o = *opts;
   if (!S->o.max_n) S->o.max_n = ~0ull;
@@ -430,6 +455,7 @@ gb_status gb_submit(gb_ctx* c, const gb_request* reqs, size_t count, uint64_t* t
     }
     const int ln = (r.kind == GB_REQ_SINGLE || r.count <= S->o.small_range) ? 0 : 1;
     S->q[ln].push_back(p);
+    S->queued[ln].fetch_add(1, std::memory_order_release);
   }
   S->cv_work.notify_all();
   return GB_OK;
@@ -496,6 +522,7 @@ gb_status gb_serve_stop(gb_ctx* c) {
   {
     std::lock_guard<std::mutex> lk(S->mu);
     S->stop = true;
+    S->stopping.store(true, std::memory_order_relaxed);
   }
   S->cv_work.notify_all();
   for (Lane& L : S->lane)

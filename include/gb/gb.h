@@ -343,7 +343,9 @@ typedef struct gb_serve_opts {
   uint64_t small_range;        /* ranges of <= this many n run n by n (0: 2^15) */
   uint32_t no_graph;           /* 1: single-lane batches of < 8192 n as plain
                                   stream launches instead of one CUDA graph   */
-  uint32_t reserved;           /* 0                                            */
+  uint32_t spin_us;            /* a lane out of work polls its queue this long
+                                  before it blocks (0: blocks at once; polling
+                                  keeps a host core busy per lane)           */
 } gb_serve_opts;
 
 typedef struct gb_serve_stats {

@@ -92,15 +92,15 @@ def test_high_offsets_match_the_oracle(gbmod, oracle):
 def test_graph_and_stream_launches_agree(gbmod):
     """Small single-lane batches run as one CUDA graph (copy sizes and kernel
     arguments updated per batch); with no_graph the same requests run as
-    plain stream launches.  Both give the same responses, one request at a
-    time (one batch each) and as a burst, and the single n match
-    gb_check_single_batch."""
+    plain stream launches; with spin_us the lanes poll their queues before
+    blocking.  All give the same responses, one request at a time (one batch
+    each) and as a burst, and the single n match gb_check_single_batch."""
     rng = np.random.default_rng(21)
     a = [int(x) * 2 for x in rng.integers(2, 2**62, size=60)] + [4, 6, 8, 100]
     out = {}
     with gbmod.Context(0) as ctx:
-        for no_graph in (False, True):
-            ctx.serve_start(small_range=2000, no_graph=no_graph)
+        for no_graph, spin in ((False, 0), (True, 0), (False, 2000)):
+            ctx.serve_start(small_range=2000, no_graph=no_graph, spin_us=spin)
             got = []
             for x in a[:20]:  # one at a time: one batch per request
                 got.append(ctx.wait(ctx.submit([0], [x], [1])[0], 60000))
@@ -108,8 +108,8 @@ def test_graph_and_stream_launches_agree(gbmod):
             burst = ctx.submit(kinds, a[20:] + [10**12], [1] * (len(a) - 20) + [500])
             got += [ctx.wait(t, 60000) for t in burst]
             assert all(g["status"] == 0 for g in got)
-            out[no_graph] = [(g["p"], g["q"], g["verified"], g["minp_sum"]) for g in got]
+            out[(no_graph, spin)] = [(g["p"], g["q"], g["verified"], g["minp_sum"]) for g in got]
             ctx.serve_stop()
         p, _, _ = ctx.check_single(np.array(a, np.uint64))
-    assert out[False] == out[True]
-    assert [o[0] for o in out[False][:len(a)]] == [int(x) for x in p]
+    assert out[(False, 0)] == out[(True, 0)] == out[(False, 2000)]
+    assert [o[0] for o in out[(False, 0)][:len(a)]] == [int(x) for x in p]
