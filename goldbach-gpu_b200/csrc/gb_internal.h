@@ -103,6 +103,7 @@ struct WinDesc {
 struct WindowsArgs {
   SearchParams s;
   const WinDesc* win;      // nwin descriptors, sorted by q_top ascending
+  const longlong2* wg;     // per descriptor: (first odd index g0, bits of its bitset)
   uint32_t nwin;
   const uint64_t* tile_off;   // nwin+1 prefix sums of bitset tiles
   const uint64_t* chunk_off;  // nwin+1 prefix sums of search chunks

@@ -80,7 +80,7 @@ namespace {
 // bytes the range lane's windows call takes from its arena for a batch
 uint64_t range_bytes(const gb_request& r) {
   const uint64_t wbits = ((32768 / 2 + r.count + 64 + 128) + 127) / 128 * 128;
-  return wbits / 8 + 96;
+  return wbits / 8 + 112;  // + descriptor, (g0, bits) record, offsets, results
 }
 
 void finish(gb_server* S, const Pending& p, gb_response& resp, uint64_t t_done) {

@@ -65,6 +65,7 @@ static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, cons
   std::vector<uint64_t> out_off(count + 1, 0);
   for (size_t i = 0; i < count; ++i) out_off[i + 1] = out_off[i] + w[i].count;
   std::vector<WinDesc> desc(count);
+  std::vector<longlong2> wg(count);  // (g0, wbits): what the large-prime pass reads
   std::vector<uint64_t> tile_off(count + 1, 0), chunk_off(count + 1, 0);
   uint64_t words = 0;
   for (size_t r = 0; r < count; ++r) {
@@ -79,6 +80,8 @@ static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, cons
     d.nsieve = 0;  // set on the device (launch_win_nsieve)
     d.orig = i;
     words += d.wbits / 32;
+    wg[r].x = (long long)(d.start >> 1) - (long long)(H >> 1);
+    wg[r].y = (long long)d.wbits;
     tile_off[r + 1] = tile_off[r] + (d.wbits + kWinTileBits - 1) / kWinTileBits;
     chunk_off[r + 1] = chunk_off[r] + (d.count + NE - 1) / NE;
   }
@@ -92,7 +95,8 @@ static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, cons
 
   Temps tmp(c, arena);
   void *d_desc, *d_toff, *d_coff, *d_bits, *d_fail, *d_maxp, *d_psum, *d_minp = nullptr;
-  if ((st = ws_buffer(c, ws, tmp, 0, count * sizeof(WinDesc), &d_desc)) != GB_OK ||
+  const size_t desc_bytes = (count * sizeof(WinDesc) + 15) / 16 * 16;
+  if ((st = ws_buffer(c, ws, tmp, 0, desc_bytes + count * sizeof(longlong2), &d_desc)) != GB_OK ||
       (st = ws_buffer(c, ws, tmp, 1, (count + 1) * 8, &d_toff)) != GB_OK ||
       (st = ws_buffer(c, ws, tmp, 2, (count + 1) * 8, &d_coff)) != GB_OK ||
       (st = ws_buffer(c, ws, tmp, 3, words * 4, &d_bits)) != GB_OK ||
@@ -119,6 +123,7 @@ static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, cons
   sp.queue = ws.queue;
   sp.queue_cap = ws.queue_cap;
   a.win = (const WinDesc*)d_desc;
+  a.wg = (const longlong2*)((char*)d_desc + desc_bytes);
   a.nwin = (uint32_t)count;
   a.tile_off = (const uint64_t*)d_toff;
   a.chunk_off = (const uint64_t*)d_coff;
@@ -140,6 +145,7 @@ static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, cons
     if (e == cudaSuccess && x != cudaSuccess) e = x;
   };
   chk(cudaMemcpyAsync(d_desc, desc.data(), count * sizeof(WinDesc), cudaMemcpyHostToDevice, s));
+  chk(cudaMemcpyAsync((void*)a.wg, wg.data(), count * sizeof(longlong2), cudaMemcpyHostToDevice, s));
   chk(launch_win_nsieve((WinDesc*)d_desc, (uint32_t)count, c->d_primes, c->nprimes, s));
   chk(cudaMemcpyAsync(d_toff, tile_off.data(), (count + 1) * 8, cudaMemcpyHostToDevice, s));
   chk(cudaMemcpyAsync(d_coff, chunk_off.data(), (count + 1) * 8, cudaMemcpyHostToDevice, s));

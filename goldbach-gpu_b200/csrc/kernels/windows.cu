@@ -135,12 +135,16 @@ __global__ void __launch_bounds__(256) win_large_kernel(const __grid_constant__ 
       w0 = lo;
       w1 = a.nwin;
     }
+    // one 16-byte load per window; the descriptor only on a hit (p is at
+    // least 2^17, the bitsets 2^13..2^25 bits: most windows get none)
+#pragma unroll 4
     for (uint32_t w = w0; w < w1; ++w) {
-      const WinDesc d = a.win[w];
-      const int64_t g0 = (int64_t)(d.start >> 1) - (int64_t)(a.s.halo >> 1);
-      const uint64_t f = first_mark_f64(g0, p, inv, gpp);
-      uint32_t* bw = a.bits + d.wbase;
-      for (uint64_t i = f; i < d.wbits; i += p) atomicAnd(&bw[i >> 5], ~(1u << (i & 31)));
+      const longlong2 v = a.wg[w];
+      const uint64_t f = first_mark_f64(v.x, p, inv, gpp);
+      if (f < (uint64_t)v.y) {
+        uint32_t* bw = a.bits + a.win[w].wbase;
+        for (uint64_t i = f; i < (uint64_t)v.y; i += p) atomicAnd(&bw[i >> 5], ~(1u << (i & 31)));
+      }
     }
   }
 }
