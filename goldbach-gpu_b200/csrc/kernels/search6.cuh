@@ -300,6 +300,13 @@ __device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_
   const uint32_t K1 = cx.K[ri][0], K5 = cx.K[ri][1];
   const uint64_t ibase = cx.base_idx + ((n0 - cx.A) >> 1);
   Cache6<kWT6> ca;
+  // without per-n output the step clears bits with one operation per word
+  // and counts the lane's unresolved n: resolved = live before - live after
+  uint32_t live = 0;
+  if (!MINP) {
+#pragma unroll
+    for (int i = 0; i < kWT6; ++i) live += __popc(U[i]);
+  }
   const uint32_t pos0 = level6_start(L), pend = level6_end(ri, L);
 #pragma unroll 1
   for (uint32_t pos = pos0; pos < pend; ++pos) {
@@ -315,7 +322,20 @@ __device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_
     const uint32_t wo = off >> 5;
     ca.at(q5 ? Q5 : Q1, wo, wo | (q5 << 31), W);
     const uint32_t p = MINP ? 6 * e6_u(e) + e6_pmod(ri, q5) : 0;
-    uint32_t cnt = step6<MINP, kWT6>(s, U, ca.lo, ca.hi, off & 31, p, W, ibase);
+    uint32_t cnt;
+    if (MINP) {
+      cnt = step6<MINP, kWT6>(s, U, ca.lo, ca.hi, off & 31, p, W, ibase);
+    } else {
+      uint32_t now = 0;
+      const uint32_t sh = off & 31;
+#pragma unroll
+      for (int i = 0; i < kWT6; ++i) {
+        U[i] &= ~__funnelshift_r(ca.lo[i], ca.hi[i], sh);
+        now += __popc(U[i]);
+      }
+      cnt = live - now;
+      live = now;
+    }
     cnt = __reduce_add_sync(0xffffffffu, cnt);
     if (lane == 0 && cnt) atomicAdd(&HIST[e6_k(e)], cnt);
   }
