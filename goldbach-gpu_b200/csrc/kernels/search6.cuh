@@ -308,6 +308,8 @@ __device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_
     for (int i = 0; i < kWT6; ++i) live += __popc(U[i]);
   }
   const uint32_t pos0 = level6_start(L), pend = level6_end(ri, L);
+  uint32_t held = 0, kheld = 0;  // a step's count waiting for the next step's
+  bool pending = false;          // (warp-uniform)
 #pragma unroll 1
   for (uint32_t pos = pos0; pos < pend; ++pos) {
     if (((pos - pos0) & 7) == 0) {
@@ -336,8 +338,24 @@ __device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_
       cnt = live - now;
       live = now;
     }
-    cnt = __reduce_add_sync(0xffffffffu, cnt);
-    if (lane == 0 && cnt) atomicAdd(&HIST[e6_k(e)], cnt);
+    // two steps' counts (at most 7 * 32 * 32 = 7168 each) share one warp
+    // reduction, packed in the two halves of a word
+    if (pending) {
+      const uint32_t v = __reduce_add_sync(0xffffffffu, held | (cnt << 16));
+      if (lane == 0) {
+        if (v & 0xffffu) atomicAdd(&HIST[kheld], v & 0xffffu);
+        if (v >> 16) atomicAdd(&HIST[e6_k(e)], v >> 16);
+      }
+      pending = false;
+    } else {
+      held = cnt;
+      kheld = e6_k(e);
+      pending = true;
+    }
+  }
+  if (pending) {
+    const uint32_t v = __reduce_add_sync(0xffffffffu, held);
+    if (lane == 0 && v) atomicAdd(&HIST[kheld], v);
   }
   if (L + 1 < kLevels6) {
     uint2* out = surv6_list(L & 1, ri);
