@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(256) win_large_kernel(const __grid_constant__ 
     }
     // one 16-byte load per window; the descriptor only on a hit (p is at
     // least 2^17, the bitsets 2^13..2^25 bits: most windows get none)
-#pragma unroll 4
+#pragma unroll 8
     for (uint32_t w = w0; w < w1; ++w) {
       const longlong2 v = a.wg[w];
       const uint64_t f = first_mark_f64(v.x, p, inv, gpp);
