@@ -65,10 +65,7 @@ struct RangeArgs {
   const uint64_t* magic;   // Barrett reciprocals, magic[k] for primes[k]
   uint32_t nsieve;         // primes[kWheelPrimeCount+1 .. nsieve) mark the window
   uint32_t kcoop;          // ... those below kcoop warp-cooperatively
-  const uint32_t* wheel;   // wheel pattern table (kWheelWords)
-  // mod-6 layout (range6_kernel): class wheel patterns, per-prime class
-  // offsets, and the bits each class bitset marks
-  int layout6;
+  // class wheel patterns and per-prime class offsets of the mod-6 layout
   const uint32_t* wheel6;  // kWheel6Words
   const uint2* a15;
   uint2* surv;             // survivor lists: 6 per CTA of surv_cap entries each

@@ -316,9 +316,8 @@ gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint
     return fail(w, GB_EINVAL, "halo must be a multiple of 64 in [128, 2^17]");
   uint32_t NE = o.chunk_evens;
   if (!NE) {
-    // the mod-6 window is 2/3 the size of the odd-only one: 2^20 n fit two
-    // CTAs per SM
-    NE = kRangeLayout6 ? 1u << 20 : 1u << 19;
+    // 2^20 n: two CTAs per SM (the two class bitsets hold 2^20 / 3 bits each)
+    NE = 1u << 20;
     while (NE > 8192 && NE / 2 >= count) NE >>= 1;
   }
   if (NE < 8192 || NE > (1u << 20) || (NE & (NE - 1)))
@@ -343,19 +342,11 @@ gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint
   a.chunks_per_seg = cps;
   a.total_items = my_segs * cps;
   a.chunk_evens = NE;
-  a.layout6 = kRangeLayout6;
-  uint64_t search_top, window_bits;
-  if (kRangeLayout6) {
-    // two class bitsets of H/6 + NE/3 bits (plus the over-read of the last
-    // warp task); primes p <= H - 13 keep every q = n - p in the window
-    a.nbw = range6_words(H, NE);
-    search_top = std::min<uint64_t>(H - 13, p_lim);
-    window_bits = H / 6 + NE / 3;
-  } else {
-    a.nbw = (H / 2 + NE) / 32 + 2;
-    search_top = std::min<uint64_t>(H - 1, p_lim);
-    window_bits = H / 2 + NE;
-  }
+  // two class bitsets of H/6 + NE/3 bits (plus the over-read of the last
+  // warp task); primes p <= H - 13 keep every q = n - p in the window
+  a.nbw = range6_words(H, NE);
+  const uint64_t search_top = std::min<uint64_t>(H - 13, p_lim);
+  const uint64_t window_bits = H / 6 + NE / 3;
   uint64_t ns = 0, kf = 0, nsv = 0, kc = 0;
   if ((st = count_le(c, w, search_top, &ns)) != GB_OK ||
       (st = count_le(c, w, o.p_small, &kf)) != GB_OK ||
@@ -377,7 +368,6 @@ gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint
   a.magic = c->d_magic;
   a.nsieve = (uint32_t)std::max<uint64_t>(nsv, kWheelPrimeCount + 1);
   a.kcoop = (uint32_t)std::max<uint64_t>(kc, kWheelPrimeCount + 1);
-  a.wheel = c->d_wheel;
   a.wheel6 = c->d_wheel6;
   a.a15 = c->d_a15;
 
@@ -434,7 +424,7 @@ gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint
   if (bps < 1) bps = 1;
   uint64_t grid = (uint64_t)c->sm_count * bps;
   if (a.total_items < grid) grid = std::max<uint64_t>(1, a.total_items);
-  if (a.layout6 && a.total_items) {  // survivor lists of the levelled search
+  if (a.total_items) {  // survivor lists of the levelled search
     a.surv_cap = a.nbw;
     void* p = nullptr;
     if ((st = ws_scratch(c, w, (size_t)grid * 6 * a.surv_cap * sizeof(uint2), &p)) != GB_OK) return st;

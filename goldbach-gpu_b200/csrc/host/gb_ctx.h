@@ -98,9 +98,6 @@ constexpr uint64_t kHostPrimeLimit = 1ull << 22;
 constexpr uint64_t kSampleStride = 1024;
 // primes searched word-parallel (lockstep) before the per-n tail
 constexpr uint64_t kLockPrimes = 128;
-// range kernel window layout: true = mod-6 class bitsets (range6_kernel),
-// false = odd-only bitset (range_kernel)
-constexpr bool kRangeLayout6 = true;
 
 gb_status fail(Workspace& w, gb_status st, const std::string& msg);
 gb_status cuda_fail(Workspace& w, cudaError_t e, const char* what);

@@ -8,11 +8,11 @@
 // and a stream sync per segment, then the host Phase 2 (:362-373).
 //
 // Each CTA takes work items (chunks of NE consecutive even n) from a global
-// counter.  For chunk [A, A+2NE) it sieves the odd q-window [A-H+1,
-// A+2NE+64) into shared memory (sieve_window.cuh) and searches it there
-// (search.cuh): the bitset never touches HBM.  n whose minimal p is >= H
-// (none below 1e12 for H >= 2^12) go to a device queue that fallback_kernel
-// serves.
+// counter.  For a chunk it sieves the q-window in the mod-6 layout (the two
+// class bitsets of the odd q not divisible by 3, sieve6.cuh) into shared
+// memory and searches it there (search6.cuh): the bitset never touches
+// HBM.  n whose minimal p is beyond the window go to a device queue that
+// fallback_kernel serves.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -27,65 +27,9 @@
 
 namespace gb {
 
-constexpr int kRangeThreads = 512;
-
-template <bool MINP>
-__global__ void __launch_bounds__(kRangeThreads, 2) range_kernel(const __grid_constant__ RangeArgs a) {
-  extern __shared__ uint32_t smem[];
-  uint32_t* pat = smem;
-  uint32_t* Q = pat + kWheelWords;
-  uint32_t* HIST = Q + a.nbw;
-  uint16_t* SOFF = reinterpret_cast<uint16_t*>(HIST + kSmemHistBins);
-  __shared__ unsigned long long s_item, s_psum;
-  __shared__ uint32_t s_fb, s_maxp;
-  const int tid = threadIdx.x;
-  const SearchParams& s = a.s;
-
-  for (uint32_t i = tid; i < kWheelWords; i += kRangeThreads) pat[i] = a.wheel[i];
-  load_search_offsets<kRangeThreads>(s, SOFF);
-
-  for (;;) {
-    if (tid == 0) {
-      s_item = atomicAdd(&s.ctr[kCtrWork], 1ull);
-      s_fb = 0;
-      s_maxp = 0;
-      s_psum = 0;
-    }
-    for (uint32_t i = tid; i < kSmemHistBins; i += kRangeThreads) HIST[i] = 0;
-    __syncthreads();
-    const unsigned long long item = s_item;
-    if (item >= a.total_items) break;
-    const uint64_t ls = item / a.chunks_per_seg;
-    const uint64_t ci = item - ls * a.chunks_per_seg;
-    const uint64_t seg = a.shard_index + ls * a.shard_count;
-    const uint64_t seg_first = seg * a.seg_size;
-    const uint64_t seg_rem = a.total_count - seg_first;
-    const uint64_t seg_cnt = seg_rem < a.seg_size ? seg_rem : a.seg_size;
-    const uint64_t j0 = ci * a.chunk_evens;
-    if (j0 >= seg_cnt) {  // past the end of a short last segment
-      __syncthreads();
-      continue;
-    }
-    Chunk c;
-    c.base_idx = seg_first + j0;
-    c.A = a.start + 2 * c.base_idx;
-    c.unit = seg;
-    c.cnt = (uint32_t)(seg_cnt - j0 < a.chunk_evens ? seg_cnt - j0 : a.chunk_evens);
-
-    // window bit i <-> odd index g0 + i, g0 = (A - H) / 2 (negative near 0)
-    const int64_t g0 = (int64_t)(c.A >> 1) - (int64_t)(s.halo >> 1);
-    const uint32_t nbits = s.halo / 2 + c.cnt + 32;
-    const uint64_t q_top = c.A + 2ull * (c.cnt - 1);  // the chunk's last n (no wrap below 2^64)
-    sieve_window<kRangeThreads>(Q, a.nbw, nbits, g0, q_top, pat, s.primes, a.magic, a.nsieve,
-                                a.kcoop);
-    search_chunk<MINP, kRangeThreads>(s, Q, SOFF, HIST, c, &s_fb, &s_maxp, &s_psum);
-  }
-}
-
 // ---------------------------------------------------------------------------
-// The same fused kernel on the mod-6 layout (sieve6.cuh, search6.cuh): the
-// q-window is the two class bitsets Q1 / Q5 (no multiple of 3 stored), and
-// the n of a chunk are searched by class n mod 6.
+// The fused kernel: the q-window is the two class bitsets Q1 / Q5 (no
+// multiple of 3 stored), and the n of a chunk are searched by class n mod 6.
 
 // threads per CTA and CTAs per SM of range6_kernel
 constexpr int kRange6Threads = 512;
@@ -244,14 +188,11 @@ uint32_t range6_words(uint32_t halo, uint32_t chunk_evens) {
 }
 
 size_t range_smem_bytes(const RangeArgs& a) {
-  if (a.layout6)
-    return range6_smem_words(a.nbw) * sizeof(uint32_t);
-  return (size_t)(kWheelWords + a.nbw + kSmemHistBins) * sizeof(uint32_t) +
-         (size_t)((a.s.nsearch + 1) & ~1u) * sizeof(uint16_t);
+  return range6_smem_words(a.nbw) * sizeof(uint32_t);
 }
 
 template <typename K>
-static int occupancy(K kernel, size_t smem, int threads = kRangeThreads) {
+static int occupancy(K kernel, size_t smem, int threads) {
   int nb = 0;
   cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, smem);
@@ -260,15 +201,13 @@ static int occupancy(K kernel, size_t smem, int threads = kRangeThreads) {
 
 int range_max_blocks_per_sm(const RangeArgs& a) {
   const size_t smem = range_smem_bytes(a);
-  if (a.layout6)
-    return a.s.minp ? occupancy(range6_kernel<true>, smem, kRange6Threads)
-                    : occupancy(range6_kernel<false>, smem, kRange6Threads);
-  return a.s.minp ? occupancy(range_kernel<true>, smem) : occupancy(range_kernel<false>, smem);
+  return a.s.minp ? occupancy(range6_kernel<true>, smem, kRange6Threads)
+                  : occupancy(range6_kernel<false>, smem, kRange6Threads);
 }
 
 template <typename K>
 static cudaError_t launch_one(K kernel, const RangeArgs& a, int grid, size_t smem, cudaStream_t st,
-                              int threads = kRangeThreads) {
+                              int threads) {
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   kernel<<<grid, threads, smem, st>>>(a);
@@ -277,11 +216,8 @@ static cudaError_t launch_one(K kernel, const RangeArgs& a, int grid, size_t sme
 
 cudaError_t launch_range(const RangeArgs& a, int grid, cudaStream_t st) {
   const size_t smem = range_smem_bytes(a);
-  if (a.layout6)
-    return a.s.minp ? launch_one(range6_kernel<true>, a, grid, smem, st, kRange6Threads)
-                    : launch_one(range6_kernel<false>, a, grid, smem, st, kRange6Threads);
-  return a.s.minp ? launch_one(range_kernel<true>, a, grid, smem, st)
-                  : launch_one(range_kernel<false>, a, grid, smem, st);
+  return a.s.minp ? launch_one(range6_kernel<true>, a, grid, smem, st, kRange6Threads)
+                  : launch_one(range6_kernel<false>, a, grid, smem, st, kRange6Threads);
 }
 
 cudaError_t launch_fallback(const SearchParams& s, int grid, cudaStream_t st) {
