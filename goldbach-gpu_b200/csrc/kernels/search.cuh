@@ -1,7 +1,7 @@
 // search.cuh -- word-parallel minimal-p search over an odd-only q-window
 // held in shared memory, used by the batched windows pipeline (windows.cu);
 // the range kernel searches the mod-6 layout instead (search6.cuh), and
-// shares this file's Chunk, histogram size and per-n bookkeeping.
+// includes this file for its shared histogram size.
 //
 // Replaces goldbach_phase1_kernel (src/goldbach.cu:288-311), which runs one
 // thread per even n, gathers one scattered bit per (n, p), divides n by 2
