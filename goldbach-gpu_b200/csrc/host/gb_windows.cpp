@@ -298,9 +298,9 @@ static gb_status windows_mr_impl(gb_ctx* c, Workspace& ws, Arena* arena, const g
 
 // Splits the batch, trading the sieve bound against Miller-Rabin: windows
 // narrower than the sieve's break-even take the Miller-Rabin path (the
-// sieve's large-prime pass costs about 2.5 ps of GPU time per sieving prime
-// per window, the single-n path about 3.8 ns per n, so the break-even width
-// is about pi(sqrt(top)) / 1500 even n; 1200 measured best on 4096 windows
+// sieve's large-prime pass costs about 1.5 ps of GPU time per sieving prime
+// per window, the single-n path about 3 ns per n, so the break-even width
+// is about pi(sqrt(top)) / 2000 even n; 2600 measured best on 4096 windows
 // in [1e15, 1e18]).  Results do not depend on the split.
 gb_status windows_impl(gb_ctx* c, Workspace& ws, Arena* arena, const gb_window* w, size_t count,
                        const gb_windows_opts* opts, gb_window_result* res, uint32_t* min_p_concat,
@@ -319,7 +319,7 @@ gb_status windows_impl(gb_ctx* c, Workspace& ws, Arena* arena, const gb_window* 
     uint64_t lim = o.mr_below;
     if (!lim) {
       const double r = std::sqrt((double)last);
-      lim = r > 1e4 ? (uint64_t)(1.1 * r / std::log(r) / 1200.0) : 0;
+      lim = r > 1e4 ? (uint64_t)(1.1 * r / std::log(r) / 2600.0) : 0;
     }
     narrow[i] = w[i].count < lim;
     nn += narrow[i];

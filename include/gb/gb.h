@@ -274,7 +274,7 @@ typedef struct gb_windows_opts {
   uint64_t mr_below;      /* windows of fewer even n skip the sieve: their q
                              are tested by Miller-Rabin (the single-n
                              kernel).  0: automatic, where sieving would
-                             cost more (about pi(sqrt(top)) / 1200 n);
+                             cost more (about pi(sqrt(top)) / 2600 n);
                              1: never                                      */
 } gb_windows_opts;
 
