@@ -164,6 +164,7 @@ def load(path: str = LIB_PATH):
                                     vp, P(WindowsSummary)]),
         "gb_now_ns": (u64, []),
         "gb_probe_peaks": (i32, [vp, P(C.c_double), P(C.c_double)]),
+        "gb_probe_mont_products": (i32, [vp, P(C.c_double)]),
         "gb_serve_start": (i32, [vp, P(ServeOpts)]),
         "gb_submit": (i32, [vp, P(Request), C.c_size_t, P(u64)]),
         "gb_poll": (i32, [vp, u64, P(Response)]),
@@ -416,6 +417,12 @@ class Context:
         a, m = C.c_double(), C.c_double()
         self._check(self.L.gb_probe_peaks(self._h, C.byref(a), C.byref(m)))
         return a.value, m.value
+
+    def probe_mont_products(self) -> float:
+        """64-bit Montgomery products per second measured on this GPU."""
+        v = C.c_double()
+        self._check(self.L.gb_probe_mont_products(self._h, C.byref(v)))
+        return v.value
 
     def now_ns(self) -> int:
         return self.L.gb_now_ns()

@@ -144,7 +144,8 @@ cudaError_t launch_win_nsieve(WinDesc* win, uint32_t nwin, const uint32_t* prime
 cudaError_t launch_window_stages(const WindowsArgs& a, uint32_t w_only, int grid_tile,
                                  int grid_large, int grid_search, cudaStream_t s, int* launches);
 
-// kernels/probe.cu: kind 0 = 32-bit ALU ops/s, 1 = shared-memory atomicAnd/s
+// kernels/probe.cu: kind 0 = 32-bit ALU ops/s, 1 = shared-memory atomicAnd/s,
+// 2 = 64-bit Montgomery products/s
 cudaError_t run_probe(int kind, int sm_count, double* ops_per_s, cudaStream_t st);
 
 // kernels/single.cu

@@ -300,6 +300,8 @@ gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint
                      const gb_range_opts* opts, gb_range_result* res, const gb_range_out* out) {
   if (limit & 1) limit--;
   if (start < 4) start = 4;
+  // an odd start rounds up; 2^64 - 1 has no even successor
+  if (start == UINT64_MAX) return fail(w, GB_EINVAL, "START must be less than LIMIT");
   if (start & 1) start++;
   if (start > limit) return fail(w, GB_EINVAL, "START must be less than LIMIT");
   gb_range_opts o{};
@@ -711,8 +713,9 @@ static gb_status sieve_bitset_impl(gb_ctx* c, Workspace& w, uint64_t q_lo, uint6
                                    uint32_t* words, int on_device, void* stream) {
   if (!words || !(q_lo & 1)) return fail(w, GB_EINVAL, "q_lo must be odd");
   if (nbits == 0) return GB_OK;
+  // the last bit's q, q_lo + 2 (nbits - 1), must not pass 2^64 - 1
+  if (nbits - 1 > (UINT64_MAX - q_lo) / 2) return fail(w, GB_EINVAL, "window passes 2^64");
   const uint64_t top = q_lo + 2 * (nbits - 1);
-  if (top < q_lo) return fail(w, GB_EINVAL, "window passes 2^64");
   const uint64_t root = isqrt_u64(top);
   gb_status st = ensure_primes(c, w, root + 2);
   if (st != GB_OK) return st;
@@ -760,6 +763,7 @@ static gb_status autotune_impl(gb_ctx* c, Workspace& w, uint64_t start, uint64_t
   gb_autotune_result r{};
   if (limit & 1) limit--;
   if (start < 4) start = 4;
+  if (start == UINT64_MAX) return fail(w, GB_EINVAL, "start must be <= limit");
   if (start & 1) start++;
   if (start > limit) return fail(w, GB_EINVAL, "start must be <= limit");
   const uint64_t count = (limit - start) / 2 + 1;
@@ -945,4 +949,11 @@ extern "C" gb_status gb_probe_peaks(gb_ctx* c, double* alu_ops_per_s, double* sm
       run_probe(1, c->sm_count, smem_atomics_per_s, c->stream) != cudaSuccess)
     return GB_ECUDA;
   return GB_OK;
+}
+
+extern "C" gb_status gb_probe_mont_products(gb_ctx* c, double* per_s) {
+  if (!c || !per_s) return GB_EINVAL;
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  return run_probe(2, c->sm_count, per_s, c->stream) == cudaSuccess ? GB_OK : GB_ECUDA;
 }

@@ -13,12 +13,15 @@
 // The array's name seen from host code is a host-side stand-in, not a
 // device address: passing it to a kernel would fault (or, where the GPU can
 // reach host memory, silently use the wrong memory).  Its device address is
-// obtained once per device with cudaGetSymbolAddress, with that device
-// current, and that address is what the kernels receive.
+// looked up with cudaGetSymbolAddress, with the device current, and that
+// address is what the kernels receive.  The table is built once per CUDA
+// context (the array is per context: a reset or another context on the
+// same device starts with it zeroed).
 #include <cuda_runtime.h>
 
 #include <cstdint>
 #include <mutex>
+#include <vector>
 
 #include "../gb_internal.h"
 #include "gb/gb.h"
@@ -81,9 +84,47 @@ __global__ void __launch_bounds__(1024) noalloc_table_kernel(unsigned char* scra
 }
 
 namespace {
+// The scratch array exists once per CUDA context: a context created later
+// on the same device (after cudaDeviceReset, or a context the caller made
+// current through the driver API) loads the module afresh, with the array
+// zeroed and possibly at another address.  Set-up is therefore cached per
+// context, keyed by the driver's context ID, which is never reused within
+// a process.
+typedef int (*CtxGetCurrentFn)(void**);
+typedef int (*CtxGetIdFn)(void*, unsigned long long*);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+std::once_flag g_entry_once;
+
+struct ScratchSetup {
+  unsigned long long ctx_id;  // driver context ID (device + 1 when IDs are unavailable)
+  void* ptr;                  // device address of g_noalloc_scratch in that context
+};
 std::mutex g_setup_mu;
-void* g_scratch_ptr[64];  // device address of g_noalloc_scratch per device
-bool g_table_ready[64];
+std::vector<ScratchSetup> g_setups;  // contexts whose table is built
+
+// ID of the context current on this thread; the device number + 1 when the
+// driver entry points cannot be had (then a reset is not detected).
+unsigned long long current_context_key(int dev) {
+  std::call_once(g_entry_once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(f);
+    cudaGetLastError();
+  });
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (g_ctx_get_current && g_ctx_get_id && g_ctx_get_current(&ctx) == 0 && ctx &&
+      g_ctx_get_id(ctx, &id) == 0)
+    return id | (1ull << 63);  // kept apart from the device-number fallback
+  return (unsigned long long)dev + 1;
+}
 }  // namespace
 
 }  // namespace gb
@@ -97,21 +138,23 @@ extern "C" gb_status gb_check_single_batch_noalloc(const uint64_t* n, size_t cou
   if (p_limit == 0) p_limit = GB_NOALLOC_P_LIMIT;
   if (p_limit > GB_NOALLOC_P_LIMIT) return GB_EINVAL;  // beyond the fixed prime table
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return GB_ENODEV;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return GB_ENODEV;
   cudaStream_t s = (cudaStream_t)stream;
   void* ptr = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_setup_mu);
-    if (!g_scratch_ptr[dev]) {
-      if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return GB_ECUDA;
-      g_scratch_ptr[dev] = ptr;
-    }
-    ptr = g_scratch_ptr[dev];
-    if (!g_table_ready[dev]) {
-      // first call on this device: build the table (synchronous)
+    // the symbol lookup also binds the runtime to the thread's context, so
+    // the key read next names the context the kernels will run in
+    if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return GB_ECUDA;
+    const unsigned long long key = current_context_key(dev);
+    bool ready = false;
+    for (const ScratchSetup& e : g_setups)
+      if (e.ctx_id == key && e.ptr == ptr) ready = true;
+    if (!ready) {
+      // first call in this context: build the table (synchronous)
       noalloc_table_kernel<<<1, 1024, 0, s>>>(static_cast<unsigned char*>(ptr));
       if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) return GB_ECUDA;
-      g_table_ready[dev] = true;
+      g_setups.push_back(ScratchSetup{key, ptr});
     }
   }
   if (!count) return GB_OK;

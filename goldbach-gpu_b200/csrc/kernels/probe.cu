@@ -1,11 +1,13 @@
 // probe.cu -- peak-throughput probes for the roofline of the integer
-// kernels: 32-bit ALU operations (funnel shift, three-input logic, add) and
-// shared-memory atomicAnd, each with independent work per thread so that
-// issue throughput, not latency, is what gets measured.
+// kernels: 32-bit ALU operations (funnel shift, three-input logic, add),
+// shared-memory atomicAnd, and 64-bit Montgomery products (the unit of the
+// Miller-Rabin work), each with independent work per thread so that issue
+// throughput, not latency, is what gets measured.
 #include <cuda_runtime.h>
 
 #include <cstdint>
 
+#include "../gb_device.cuh"
 #include "../gb_internal.h"
 
 namespace gb {
@@ -46,6 +48,23 @@ __global__ void __launch_bounds__(256) probe_atom_kernel(uint32_t* sink, int ite
   if (s[threadIdx.x] == 0x12345u) sink[0] = s[threadIdx.x];
 }
 
+// 4 independent chains of mont_mul32 per thread (the product the single-n
+// and Phase-2 kernels use), modulus an odd 64-bit number per thread.
+__global__ void __launch_bounds__(256) probe_mont_kernel(uint32_t* sink, int iters) {
+  const uint64_t n = 0xfffffffffffffc5ull - 2ull * (blockIdx.x * 256u + threadIdx.x);  // odd
+  const Mont M = mont_init(n);
+  const uint32_t ni = (uint32_t)M.ninv;
+  uint64_t a = M.one, b = n >> 1, c = n / 3, d = n / 5;
+#pragma unroll 2
+  for (int i = 0; i < iters; ++i) {
+    a = mont_mul32(a, b, n, ni);
+    b = mont_mul32(b, c, n, ni);
+    c = mont_mul32(c, d, n, ni);
+    d = mont_mul32(d, a, n, ni);
+  }
+  if ((a ^ b ^ c ^ d) == 0x7fffffffull) sink[0] = 1;  // keeps the chains alive
+}
+
 cudaError_t run_probe(int kind, int sm_count, double* ops_per_s, cudaStream_t st) {
   uint32_t* sink = nullptr;
   cudaError_t e = cudaMalloc(&sink, 4);
@@ -53,12 +72,14 @@ cudaError_t run_probe(int kind, int sm_count, double* ops_per_s, cudaStream_t st
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  const int grid = sm_count * 8, block = 256, iters = 1 << 14;
-  const double per_thread = kind == 0 ? 8.0 * iters : (double)iters;
+  const int grid = sm_count * 8, block = 256;
+  const int iters = kind == 2 ? 1 << 11 : 1 << 14;
+  const double per_thread = kind == 0 ? 8.0 * iters : kind == 2 ? 4.0 * iters : (double)iters;
   for (int rep = 0; rep < 2; ++rep) {  // the first run warms up
     cudaEventRecord(e0, st);
     if (kind == 0) probe_alu_kernel<<<grid, block, 0, st>>>(sink, iters);
-    else probe_atom_kernel<<<grid, block, 0, st>>>(sink, iters);
+    else if (kind == 1) probe_atom_kernel<<<grid, block, 0, st>>>(sink, iters);
+    else probe_mont_kernel<<<grid, block, 0, st>>>(sink, iters);
     cudaEventRecord(e1, st);
   }
   e = cudaEventSynchronize(e1);

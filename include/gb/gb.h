@@ -242,8 +242,11 @@ gb_status gb_check_single_batch(gb_ctx* ctx, const uint64_t* n, size_t count,
  *     prime below 2^16, which is the reach of the fixed table); a larger
  *     p_limit returns GB_EINVAL.  Results equal gb_check_single_batch with
  *     the same p_limit.
- *   - The first call on each device builds the table and synchronises
- *     `stream`; make that first call before any stream capture.
+ *   - The first call in each CUDA context builds the table and
+ *     synchronises `stream`: the first call on a device, and again the
+ *     first call after cudaDeviceReset or from another context made
+ *     current on the same device.  Make that call before any stream
+ *     capture.
  *   - Later calls are asynchronous on `stream` (cudaStream_t, NULL: legacy
  *     default stream); the counters are cleared on every call.
  *   - All calls share the one array: calls that overlap on the GPU (two
@@ -360,6 +363,10 @@ typedef struct gb_serve_stats {
  * operations per second and conflict-free shared-memory atomicAnd per second
  * on this device (short probe kernels; no counterpart in the reference). */
 gb_status gb_probe_peaks(gb_ctx* ctx, double* alu_ops_per_s, double* smem_atomics_per_s);
+/* Measured peak of 64-bit Montgomery products per second (a*b*2^-64 mod n,
+ * independent products on every thread): the unit of the Miller-Rabin work
+ * in the single-n and Phase-2 kernels.  No counterpart in the reference. */
+gb_status gb_probe_mont_products(gb_ctx* ctx, double* per_s);
 
 /* Monotonic clock used for arrival times (nanoseconds). */
 uint64_t gb_now_ns(void);

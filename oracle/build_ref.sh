@@ -16,7 +16,8 @@
 # x86-64 host.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${GB_REFERENCE_DIR:-/root/reference}"
+# the reference checkout: GB_REFERENCE_DIR, else a sibling of the repository
+REF="${GB_REFERENCE_DIR:-$HERE/../../reference}"
 OUT="$HERE/_ref"
 if [ ! -d "$REF/src" ]; then
   echo "build_ref.sh: reference sources not found at $REF; keeping prebuilt $OUT" >&2

@@ -276,6 +276,16 @@ uint64_t gbo_phase2_minp(uint64_t n, uint64_t limit) {
 #define ORACLE_HALO 65536ULL
 #define ORACLE_BLOCK 65536ULL
 
+/* Evens per block: 2^16, doubled while the block is under a quarter of the
+ * sieving-prime count (up to 2^23), so that far from 0 (primes to 1e9
+ * near 1e18) the per-prime offset of segmented_sieve.cpp:39-43 is paid once
+ * per 2^23 n and not per 2^16.  Results do not depend on the block size. */
+static uint64_t oracle_block(uint64_t nbase) {
+  uint64_t blk = ORACLE_BLOCK;
+  while (blk < (1ULL << 23) && blk < nbase / 4) blk <<= 1;
+  return blk;
+}
+
 int gbo_minp_range(uint64_t start, uint64_t count, uint64_t p_limit,
                    uint32_t* minp_out, int nthreads) {
   if (count == 0) return 0;
@@ -291,12 +301,13 @@ int gbo_minp_range(uint64_t start, uint64_t count, uint64_t p_limit,
   prime_cache(p_limit > ORACLE_HALO ? p_limit : ORACLE_HALO, &nbig);
   prime_cache(p_limit, &nbig_lim);
   const uint64_t* base = big;
-  uint64_t nblk = (count + ORACLE_BLOCK - 1) / ORACLE_BLOCK;
+  const uint64_t BLK = oracle_block(nbase);
+  uint64_t nblk = (count + BLK - 1) / BLK;
   int nt = pick_threads(nthreads);
   int err = 0;
 #pragma omp parallel num_threads(nt)
   {
-    uint8_t* win = (uint8_t*)malloc(2 * ORACLE_BLOCK + ORACLE_HALO + 8);
+    uint8_t* win = (uint8_t*)malloc(2 * BLK + ORACLE_HALO + 8);
     if (!win) {
 #pragma omp atomic write
       err = 1;
@@ -304,8 +315,8 @@ int gbo_minp_range(uint64_t start, uint64_t count, uint64_t p_limit,
 #pragma omp for schedule(dynamic, 1)
     for (long long b = 0; b < (long long)nblk; b++) {
       if (!win) continue;
-      uint64_t j0 = (uint64_t)b * ORACLE_BLOCK;
-      uint64_t cnt = count - j0 < ORACLE_BLOCK ? count - j0 : ORACLE_BLOCK;
+      uint64_t j0 = (uint64_t)b * BLK;
+      uint64_t cnt = count - j0 < BLK ? count - j0 : BLK;
       uint64_t A = start + 2 * j0;
       uint64_t B = A + 2 * (cnt - 1);
       uint64_t wlo = A > H + 2 ? A - H : 2;
@@ -347,24 +358,37 @@ int gbo_minp_windows(const uint64_t* start, const uint64_t* count, size_t nwin,
   for (size_t i = 0; i < nwin; i++) {
     if (start[i] < 4 || (start[i] & 1) || !count[i]) return -1;
     uint64_t last = start[i] + 2 * (count[i] - 1);
+    if (last < start[i]) return -1;
     if (last > qmax) qmax = last;
-    nblk += (count[i] + ORACLE_BLOCK - 1) / ORACLE_BLOCK;
   }
   uint64_t need = p_limit > ORACLE_HALO ? p_limit : ORACLE_HALO;
   if (gbo_isqrt(qmax) > need) need = gbo_isqrt(qmax);
   size_t tmp = 0;
   prime_cache(need, &tmp); /* build the shared tables once, before the threads */
+  /* each window in blocks of gbo_minp_range's own size for its top */
+  uint64_t* wblk = (uint64_t*)malloc((nwin ? nwin : 1) * sizeof(uint64_t));
+  if (!wblk) return -1;
+  for (size_t i = 0; i < nwin; i++) {
+    size_t nb = 0;
+    prime_cache(gbo_isqrt(start[i] + 2 * (count[i] - 1)), &nb);
+    wblk[i] = oracle_block(nb);
+    nblk += (count[i] + wblk[i] - 1) / wblk[i];
+  }
   uint64_t* bw = (uint64_t*)malloc(nblk * sizeof(uint64_t) * 3);
-  if (!bw) return -1;
+  if (!bw) {
+    free(wblk);
+    return -1;
+  }
   uint64_t b = 0, off = 0;
   for (size_t i = 0; i < nwin; i++) {
-    for (uint64_t j0 = 0; j0 < count[i]; j0 += ORACLE_BLOCK, b++) {
+    for (uint64_t j0 = 0; j0 < count[i]; j0 += wblk[i], b++) {
       bw[3 * b] = start[i] + 2 * j0;
-      bw[3 * b + 1] = count[i] - j0 < ORACLE_BLOCK ? count[i] - j0 : ORACLE_BLOCK;
+      bw[3 * b + 1] = count[i] - j0 < wblk[i] ? count[i] - j0 : wblk[i];
       bw[3 * b + 2] = off + j0;
     }
     off += count[i];
   }
+  free(wblk);
   int err = 0;
   int nt = pick_threads(nthreads);
 #pragma omp parallel for num_threads(nt) schedule(dynamic, 1) reduction(| : err)

@@ -12,7 +12,8 @@ Sources of truth, in order of authority:
     no runnable equivalent (minimal p over [4, 1e9]) and itself pinned by the
     fixtures above.
 
-Usage: python tests/golden/make_golden.py   (needs oracle/_ref built)
+Usage: python tests/golden/make_golden.py [c1]   (needs oracle/_ref built;
+"c1" writes only ref_c1_1e9.json, about a minute of reference CPU time)
 """
 import ctypes as C
 import hashlib
@@ -143,5 +144,37 @@ def main():
     print("golden fixtures written to", GOLD)
 
 
+def make_c1():
+    """C1 as the benchmark states it: every even n in [4, 1e9].  The minimal p
+    of all 499,999,999 n by the reference's segmented_sieve + the
+    goldbach_verify scan rule (gbref_window_verify, halo 2^16: every minimal
+    p below 1e9 is under 2^11), hashed as uint32 little-endian, and the
+    verified bitmap (bit j <-> n = 4 + 2j, packed into uint32 words); plus the
+    summary the reference's cpu_goldbach binary prints for LIMIT = 1e9."""
+    R = lib(os.path.join(REF, "libgbref.so"))
+    R.gbref_window_verify.restype = C.c_uint64
+    R.gbref_window_verify.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p, C.c_int]
+    count = (10**9 - 4) // 2 + 1
+    mp = np.zeros(count, np.uint32)
+    unver = R.gbref_window_verify(4, count, 1 << 16, mp.ctypes.data, os.cpu_count() or 1)
+    bits = np.packbits(mp > 0, bitorder="little")
+    words = (count + 31) // 32
+    bits = np.concatenate([bits, np.zeros(4 * words - len(bits), np.uint8)])
+    txt = subprocess.run([os.path.join(REF, "cpu_goldbach"), str(10**9)], capture_output=True,
+                         text=True, check=True).stdout
+    json.dump({"source": "reference segmented_sieve + cpu_goldbach.cpp:19-21 scan rule over [4, 1e9] "
+                         "(oracle/_ref/libgbref.so gbref_window_verify); cpu_goldbach 1000000000 summary",
+               "start": 4, "limit": 10**9, "checked": count, "unverified": int(unver),
+               "min_p_sha256": hashlib.sha256(mp.tobytes()).hexdigest(),
+               "verified_bits_sha256": hashlib.sha256(bits.tobytes()).hexdigest(),
+               "max_minp": int(mp.max()),
+               "cpu_goldbach_checked": int(re.search(r"Even numbers checked : (\d+)", txt).group(1)),
+               "cpu_goldbach_failures": int(re.search(r"Failures found\s+: (\d+)", txt).group(1)),
+               "cpu_goldbach_final": [l for l in txt.splitlines() if "satisfy Goldbach" in l][0]},
+              open(os.path.join(GOLD, "ref_c1_1e9.json"), "w"), indent=1)
+    print("C1 fixture written to", GOLD)
+
+
 if __name__ == "__main__":
-    sys.exit(main())
+    # no argument: every fixture; "c1": only the [4, 1e9] per-n fixture
+    sys.exit(make_c1() if sys.argv[1:] == ["c1"] else (main() or make_c1()))

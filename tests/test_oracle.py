@@ -138,3 +138,17 @@ def test_published_single_check_partitions_bound_minp(oracle):
     for n, p in zip(pub, mp):
         assert 0 < p <= pub[n]
         assert oracle.mr7(int(p)) and oracle.mr7(n - int(p))
+
+
+def test_minp_over_c1_matches_reference_hash(oracle):
+    # [4, 1e9] whole (C1): the oracle's minimal p of all 499,999,999 n and the
+    # verified bitmap hash to what the reference's own scan produced
+    import hashlib
+    g = gold("ref_c1_1e9.json")
+    count = g["checked"]
+    mp = oracle.minp(4, count)
+    assert hashlib.sha256(mp.tobytes()).hexdigest() == g["min_p_sha256"]
+    bits = np.packbits(mp > 0, bitorder="little")
+    bits = np.concatenate([bits, np.zeros(4 * ((count + 31) // 32) - len(bits), np.uint8)])
+    assert hashlib.sha256(bits.tobytes()).hexdigest() == g["verified_bits_sha256"]
+    assert int(mp.max()) == g["max_minp"] and g["cpu_goldbach_failures"] == 0
