@@ -223,11 +223,25 @@ def measure_windows(gb, ctx):
     same = per == per_p
     pv = total / (sp["device_ms"] / 1e3)
     v = total / (s["device_ms"] / 1e3)
+    # roofline of the large-prime pass: one first-multiple computation (the
+    # range model's OPS_PER_OFFSET ALU ops) per (prime, window) pair it visits
+    alu_peak, _ = ctx.probe_peaks()
+    large_s = s["large_ms"] / 1e3
+    ops = s["large_pairs"] * OPS_PER_OFFSET
     return {"windows": len(starts), "even_n": total, "persistent_ms": s["device_ms"],
             "persistent_value": v, "persistent_launches": s["kernel_launches"],
             "plain_windows": len(starts), "plain_ms": sp["device_ms"], "plain_value": pv,
             "plain_launches": sp["kernel_launches"], "batched_over_plain": v / pv,
             "identical_results": bool(same), "failures": s["failures"],
+            "sieved_windows": s["sieved_windows"], "large_pairs": s["large_pairs"],
+            "large_ms": s["large_ms"], "search_ms": s["search_ms"],
+            "roofline": {"bound": "int", "kernel": "win_large_kernel",
+                         "achieved": ops / large_s / 1e12 if large_s else None,
+                         "peak": alu_peak / 1e12, "unit": "Top/s",
+                         "frac": ops / large_s / alu_peak if large_s else None,
+                         "pairs_per_s": s["large_pairs"] / large_s if large_s else None,
+                         "work_source": "(prime, window) pairs x 8 ALU ops per first-multiple computation",
+                         "peak_source": "measured in-process: gb_probe_peaks (32-bit ALU ops/s)"},
             "wall_s": wall, "plain_wall_s": wall_p, "unit": UNIT}
 
 

@@ -97,7 +97,8 @@ class WindowResult(C.Structure):
 
 class WindowsSummary(C.Structure):
     _fields_ = [("total_n", u64), ("failures", u64), ("kernel_launches", u64),
-                ("device_ms", C.c_double)]
+                ("device_ms", C.c_double), ("sieved_windows", u64), ("large_pairs", u64),
+                ("large_ms", C.c_double), ("search_ms", C.c_double)]
 
 
 class Request(C.Structure):

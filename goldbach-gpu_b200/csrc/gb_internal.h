@@ -33,7 +33,6 @@ struct QEntry {
 struct SearchParams {
   uint32_t halo;     // H: window holds q >= A - H + 1; primes p < H searched there
   uint32_t nsearch;  // primes[1 .. nsearch) searched in the window (all p <= min(H-1, p_lim))
-  uint32_t klock;    // lockstep (word-parallel) phase covers k < klock
   uint32_t kfb;      // first k whose prime exceeds p_small
   uint64_t p_lim;    // candidate bound max(p_small, phase2_limit)
   uint64_t p_small;
@@ -50,6 +49,33 @@ struct SearchParams {
   uint32_t* vbits;                // nullable: verified bits, prefilled with ones
   QEntry* queue;
   uint32_t queue_cap;
+};
+
+// Batched windows (mod-6 layout).  Window w covers the even n = start + 2j,
+// j < count.  Its large-prime mask is two class bitsets, L1 then L5, of
+// lwords words each at word lbase of the mask buffer: bit t of class c <->
+// q = 6(g0 + t) + c, with g0 = floor((start - H - 1) / 6) the first chunk's
+// window base.  A bit is cleared when q is a multiple of a sieving prime
+// above the chunk sieve's bound (other than the prime itself).
+struct WinDesc6 {
+  uint64_t start;
+  uint64_t count;
+  uint64_t out_off;  // output index of its first n
+  uint64_t q_top;    // largest n of the window (bounds the sieving primes)
+  int64_t g0;        // window base of the mask
+  uint64_t lbase;    // first word of L1 (L5 follows at lbase + lwords)
+  uint32_t lwords;   // words of each class mask
+  uint32_t orig;     // index of the window in the caller's order
+};
+
+// What the large-prime pass reads for every (prime, window) pair: the mask
+// base g0 as a double (rounded) and its low 32 bits, and the bits of each
+// class mask -- or ~0u for a window whose q may include a sieving prime
+// itself (g0 < 2^30), which takes the exact path.
+struct __align__(16) WinLarge {
+  double gd;
+  uint32_t gl;
+  uint32_t lbits;
 };
 
 struct RangeArgs {
@@ -70,6 +96,14 @@ struct RangeArgs {
   const uint2* a15;
   uint2* surv;             // survivor lists: 6 per CTA of surv_cap entries each
   uint32_t surv_cap;       // >= words of one class bitset
+  // windows mode (win != nullptr): the work items are the chunks of the
+  // windows (chunk_off: nwin + 1 prefix sums), each window's outputs are
+  // accounted to its caller index, and every chunk's q-window is ANDed with
+  // the window's large-prime mask
+  const WinDesc6* win;
+  const uint64_t* chunk_off;
+  uint32_t nwin;
+  const uint32_t* lmask;
 };
 
 struct SieveArgs {
@@ -82,38 +116,6 @@ struct SieveArgs {
   uint32_t kcoop;
   const uint32_t* wheel;
   uint32_t* out;           // ceil(nbits/32) words
-};
-
-// Batched windows: window w covers even n = start[w] + 2j, j < count[w]; its
-// q-bitset (odd q >= start - H + 1) has wbits[w] bits at word wbase[w].
-struct WinDesc {
-  uint64_t start;
-  uint64_t count;
-  uint64_t out_off;    // output index of its first n
-  uint64_t wbase;      // first word of its bitset in the global buffer
-  uint64_t wbits;      // bits of its bitset (H/2 + count + 64, rounded to 32)
-  uint64_t q_top;      // largest odd q of its bitset
-  uint32_t nsieve;     // primes[.. nsieve) needed by this window (p^2 <= q_top)
-  uint32_t orig;       // index of the window in the caller's order
-};
-
-struct WindowsArgs {
-  SearchParams s;
-  const WinDesc* win;      // nwin descriptors, sorted by q_top ascending
-  const longlong2* wg;     // per descriptor: (first odd index g0, bits of its bitset)
-  uint32_t nwin;
-  const uint64_t* tile_off;   // nwin+1 prefix sums of bitset tiles
-  const uint64_t* chunk_off;  // nwin+1 prefix sums of search chunks
-  uint64_t total_tiles, total_chunks;
-  uint32_t tile_bits;      // sieve tile (bits)
-  uint32_t chunk_evens;    // NE of the search
-  uint32_t nbw;            // shared words of a search window
-  uint32_t* bits;          // global window bitsets
-  const uint64_t* magic;
-  uint32_t nsmall;         // primes[.. nsmall) are marked in the tile sieve
-  uint32_t kcoop;
-  uint32_t nlarge;         // primes[nsmall .. nlarge) marked by the large-prime pass
-  const uint32_t* wheel;
 };
 
 // kernels/tables.cu
@@ -137,12 +139,25 @@ int range_max_blocks_per_sm(const RangeArgs& a);
 cudaError_t launch_range(const RangeArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_fallback(const SearchParams& s, int grid, cudaStream_t st);
 
-// kernels/windows.cu: the three stages for all windows (w_only = ~0u) or for
-// one window; grids are chosen by the caller.
-cudaError_t launch_win_nsieve(WinDesc* win, uint32_t nwin, const uint32_t* primes, uint64_t nprimes,
-                              cudaStream_t s);
-cudaError_t launch_window_stages(const WindowsArgs& a, uint32_t w_only, int grid_tile,
-                                 int grid_large, int grid_search, cudaStream_t s, int* launches);
+// kernels/windows.cu: the large-prime pass of the batched windows.  Primes
+// primes[k0 .. k1) (each below 2^32) clear their multiples in the class masks
+// of windows [w_lo, w_hi) of `win` / `wl` (sorted by q_top ascending); a
+// prime visits only the windows with q_top >= p^2.
+struct WinLargeArgs {
+  const WinDesc6* win;
+  const WinLarge* wl;
+  uint32_t w_lo, w_hi;
+  const uint32_t* primes;
+  const uint64_t* magic;
+  const uint2* a15;
+  uint32_t k0, k1;
+  uint32_t* lmask;
+};
+cudaError_t launch_win_large(const WinLargeArgs& a, int grid, cudaStream_t s);
+// Adds the (prime, window) pairs the pass visits (primes from index k0 up to
+// isqrt(q_top) of each window) to *pairs.
+cudaError_t launch_win_pairs(const WinDesc6* win, uint32_t nwin, const uint32_t* primes, uint64_t nprimes,
+                             uint32_t k0, unsigned long long* pairs, cudaStream_t s);
 
 // kernels/probe.cu: kind 0 = 32-bit ALU ops/s, 1 = shared-memory atomicAnd/s,
 // 2 = 64-bit Montgomery products/s

@@ -94,7 +94,8 @@ gb_status ws_init(gb_ctx* c, Workspace& w, uint32_t queue_cap) {
   if (cudaMallocHost((void**)&w.h_stage, (kCtrCount + GB_HIST_BINS) * 8) != cudaSuccess)
     return fail(w, GB_ENOMEM, "pinned staging buffer");
   if (cudaEventCreate(&w.ev0) != cudaSuccess || cudaEventCreate(&w.ev1) != cudaSuccess ||
-      cudaEventCreate(&w.ek0) != cudaSuccess || cudaEventCreate(&w.ek1) != cudaSuccess)
+      cudaEventCreate(&w.ek0) != cudaSuccess || cudaEventCreate(&w.ek1) != cudaSuccess ||
+      cudaEventCreate(&w.ek2) != cudaSuccess)
     return fail(w, GB_ECUDA, "cudaEventCreate");
   return GB_OK;
 }
@@ -144,7 +145,7 @@ void ws_free(gb_ctx* c, Workspace& w) {
   w.queue = nullptr;
   w.scratch = nullptr;
   w.scratch_bytes = 0;
-  for (cudaEvent_t* e : {&w.ev0, &w.ev1, &w.ek0, &w.ek1})
+  for (cudaEvent_t* e : {&w.ev0, &w.ev1, &w.ek0, &w.ek1, &w.ek2})
     if (*e) {
       cudaEventDestroy(*e);
       *e = nullptr;
@@ -357,7 +358,6 @@ gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint
     return st;
   sp.halo = H;
   sp.nsearch = (uint32_t)ns;
-  sp.klock = (uint32_t)std::min<uint64_t>(ns, kLockPrimes);
   sp.kfb = (uint32_t)std::min<uint64_t>(kf, 0xffffffffu);
   sp.p_lim = p_lim;
   sp.p_small = o.p_small;

@@ -44,7 +44,7 @@ struct Workspace {
   unsigned long long* hist = nullptr;  // GB_HIST_BINS
   QEntry* queue = nullptr;
   uint32_t queue_cap = 0;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ek0 = nullptr, ek1 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ek0 = nullptr, ek1 = nullptr, ek2 = nullptr;
   void* scratch = nullptr;  // per-call kernel scratch, grown on demand
   size_t scratch_bytes = 0;
   // per-call device buffers of the public entry points (slot i grown on
@@ -97,7 +97,6 @@ namespace gb {
 constexpr uint64_t kHostPrimeLimit = 1ull << 22;
 constexpr uint64_t kSampleStride = 1024;
 // primes searched word-parallel (lockstep) before the per-n tail
-constexpr uint64_t kLockPrimes = 128;
 
 gb_status fail(Workspace& w, gb_status st, const std::string& msg);
 gb_status cuda_fail(Workspace& w, cudaError_t e, const char* what);

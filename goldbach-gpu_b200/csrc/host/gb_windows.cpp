@@ -3,10 +3,12 @@
 // Many independent windows of consecutive even n (e.g. 4096 windows at
 // offsets in [1e15, 1e18]) in one batch.  The reference has no batch mode:
 // each window would be one `goldbach --start=A LIMIT` process with its own
-// segment loop (src/goldbach.cu:420-485).  GB_WINDOWS_PERSISTENT runs each
-// stage of kernels/windows.cu once over the whole batch; GB_WINDOWS_PLAIN
-// runs the same stages window by window with per-window grids (the plain
-// per-window pipeline, kept for comparison).
+// segment loop (src/goldbach.cu:420-485).  GB_WINDOWS_PERSISTENT runs the
+// batch as three launches: the large-prime pass over every window's class
+// masks (kernels/windows.cu), range6_kernel in windows mode over every
+// (window, chunk) item from one device work counter, and the device Phase 2.
+// GB_WINDOWS_PLAIN runs the same launches window by window (the per-window
+// launch pipeline, kept for comparison).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -16,17 +18,23 @@
 #include "gb_ctx.h"
 
 namespace gb {
-constexpr uint32_t kWinTileBits = 1u << 18;
-// CTAs per SM of the large-prime pass (grid-stride over the primes; a finer
-// grid evens out primes that visit many windows and primes that visit few:
-// 16 -> 64 took 4096 windows from 277 to 260 ms, 128 measured 264 ms)
+// Primes up to this bound sieve each chunk's q-window in shared memory; the
+// larger ones go through the large-prime pass (kernels/windows.cu), whose
+// quotient estimate needs p > 2^17.
+constexpr uint64_t kWinChunkSieveBound = 1ull << 20;
+// CTAs per SM of the large-prime pass (grid-stride over the primes: a fine
+// grid evens out primes that visit many windows and primes that visit few)
 constexpr uint64_t kLargeBlocksPerSM = 64;
-constexpr uint64_t kWinSmallPrimeBound = 1ull << 17;  // tile sieve marks primes below this
-}  // namespace gb
+// Default break-even divisor of the Miller-Rabin split (see windows_impl).
+constexpr double kMrBelowDivisor = 2600.0;
 
-namespace gb {
+// floor((A - H - 1) / 6) for A possibly below H (range.cu window_g0)
+static int64_t host_window_g0(uint64_t A, uint32_t H) {
+  if (A >= (uint64_t)H + 1) return (int64_t)((A - H - 1) / 6);
+  return -(int64_t)(((uint64_t)H + 1 - A + 5) / 6);
+}
 
-// The sieve pipeline over windows w[0..count) (stages of kernels/windows.cu).
+// The sieve pipeline over windows w[0..count).
 static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, const gb_window* w,
                                     size_t count, const gb_windows_opts* opts, gb_window_result* res,
                                     uint32_t* min_p_concat, gb_windows_summary* sum) {
@@ -36,14 +44,12 @@ static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, cons
   if (o.mode != GB_WINDOWS_PERSISTENT && o.mode != GB_WINDOWS_PLAIN)
     return fail(ws, GB_EINVAL, "unknown windows mode");
   if (o.on_device) return fail(ws, GB_EINVAL, "windows: on_device outputs are not supported");
-  if (count == 0) {
-    if (sum) std::memset(sum, 0, sizeof *sum);
-    return GB_OK;
-  }
+  if (sum) std::memset(sum, 0, sizeof *sum);
+  if (count == 0) return GB_OK;
   if (count > 0xffffffffull) return fail(ws, GB_EINVAL, "too many windows");
   const uint32_t H = o.halo ? o.halo : 32768u;
   if (H < 128 || H > (1u << 17) || (H & 63)) return fail(ws, GB_EINVAL, "halo must be a multiple of 64 in [128, 2^17]");
-  const uint32_t NE = o.chunk_evens ? o.chunk_evens : (1u << 19);
+  const uint32_t NE = o.chunk_evens ? o.chunk_evens : (1u << 20);
   if (NE < 8192 || NE > (1u << 20) || (NE & (NE - 1)))
     return fail(ws, GB_EINVAL, "chunk_evens must be a power of two in [2^13, 2^20]");
   const uint64_t p_lim = o.phase2_limit ? o.phase2_limit : GB_PHASE2_LIMIT_DEFAULT;
@@ -53,14 +59,16 @@ static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, cons
     if (w[i].start < 4 || (w[i].start & 1) || w[i].count == 0)
       return fail(ws, GB_EINVAL, "window start must be even and >= 4, count >= 1");
     const uint64_t last = w[i].start + 2 * (w[i].count - 1);
-    if (w[i].count > (1ull << 40) || last < w[i].start) return fail(ws, GB_EINVAL, "window passes 2^64");
+    if (w[i].count > GB_WINDOW_MAX_COUNT) return fail(ws, GB_EINVAL, "window wider than GB_WINDOW_MAX_COUNT");
+    if (last < w[i].start) return fail(ws, GB_EINVAL, "window passes 2^64");
     q_max = std::max(q_max, last);
     total_n += w[i].count;
   }
   const uint64_t root = isqrt_u64(q_max);
-  gb_status st = ensure_primes(c, ws, std::max<uint64_t>({p_lim, (uint64_t)H, root + 2, kWinSmallPrimeBound}));
+  gb_status st = ensure_primes(c, ws, std::max<uint64_t>({p_lim, (uint64_t)H, root + 2, kWinChunkSieveBound}));
   if (st != GB_OK) return st;
-  // descriptors, sorted by top q so the large-prime pass visits a suffix
+  const uint32_t nbw = range6_words(H, NE);
+  // descriptors, sorted by top q so that a prime visits a suffix of them
   std::vector<uint32_t> order(count);
   std::iota(order.begin(), order.end(), 0u);
   std::sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
@@ -68,52 +76,57 @@ static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, cons
   });
   std::vector<uint64_t> out_off(count + 1, 0);
   for (size_t i = 0; i < count; ++i) out_off[i + 1] = out_off[i] + w[i].count;
-  std::vector<WinDesc> desc(count);
-  std::vector<longlong2> wg(count);  // (g0, wbits): what the large-prime pass reads
-  std::vector<uint64_t> tile_off(count + 1, 0), chunk_off(count + 1, 0);
-  uint64_t words = 0;
+  std::vector<WinDesc6> desc(count);
+  std::vector<WinLarge> wl(count);
+  std::vector<uint64_t> chunk_off(count + 1, 0), chunk_one(2 * count, 0);
+  uint64_t lwords_total = 0;
   for (size_t r = 0; r < count; ++r) {
     const uint32_t i = order[r];
-    WinDesc& d = desc[r];
+    WinDesc6& d = desc[r];
     d.start = w[i].start;
     d.count = w[i].count;
     d.out_off = out_off[i];
-    d.wbase = words;
-    d.wbits = ((H / 2 + d.count + 64 + 128) + 127) / 128 * 128;  // slack for 16-byte loads
     d.q_top = d.start + 2 * (d.count - 1);
-    d.nsieve = 0;  // set on the device (launch_win_nsieve)
+    d.g0 = host_window_g0(d.start, H);
     d.orig = i;
-    words += d.wbits / 32;
-    wg[r].x = (long long)(d.start >> 1) - (long long)(H >> 1);
-    wg[r].y = (long long)d.wbits;
-    tile_off[r + 1] = tile_off[r] + (d.wbits + kWinTileBits - 1) / kWinTileBits;
-    chunk_off[r + 1] = chunk_off[r] + (d.count + NE - 1) / NE;
+    const uint64_t chunks = (d.count + NE - 1) / NE;
+    const int64_t g_last = host_window_g0(d.start + 2 * (uint64_t)NE * (chunks - 1), H);
+    // every chunk reads nbw + 1 mask words from its own base on
+    const uint64_t lw = ((uint64_t)(g_last - d.g0) >> 5) + nbw + 2;
+    d.lwords = (uint32_t)((lw + 3) & ~3ull);
+    d.lbase = lwords_total;
+    lwords_total += 2ull * d.lwords;
+    wl[r].gd = (double)d.g0;
+    wl[r].gl = (uint32_t)(uint64_t)d.g0;
+    wl[r].lbits = d.g0 >= (int64_t)(1ll << 30) ? d.lwords * 32 : 0xffffffffu;
+    chunk_off[r + 1] = chunk_off[r] + chunks;
+    chunk_one[2 * r + 1] = chunks;
   }
   uint64_t ns = 0, kf = 0, nsmall = 0, nlarge = 0, kc = 0;
-  if ((st = count_le(c, ws, std::min<uint64_t>(H - 1, p_lim), &ns)) != GB_OK ||
+  if ((st = count_le(c, ws, std::min<uint64_t>(H - 13, p_lim), &ns)) != GB_OK ||
       (st = count_le(c, ws, p_lim, &kf)) != GB_OK ||
-      (st = count_le(c, ws, kWinSmallPrimeBound, &nsmall)) != GB_OK ||
+      (st = count_le(c, ws, std::min<uint64_t>(kWinChunkSieveBound, root), &nsmall)) != GB_OK ||
       (st = count_le(c, ws, root, &nlarge)) != GB_OK ||
-      (st = count_le(c, ws, kWinTileBits / 64, &kc)) != GB_OK)
+      (st = count_le(c, ws, (H / 6 + NE / 3) / 64, &kc)) != GB_OK)
     return st;
 
   Temps tmp(c, arena);
-  void *d_desc, *d_toff, *d_coff, *d_bits, *d_fail, *d_maxp, *d_psum, *d_minp = nullptr;
-  const size_t desc_bytes = (count * sizeof(WinDesc) + 15) / 16 * 16;
-  if ((st = ws_buffer(c, ws, tmp, 0, desc_bytes + count * sizeof(longlong2), &d_desc)) != GB_OK ||
-      (st = ws_buffer(c, ws, tmp, 1, (count + 1) * 8, &d_toff)) != GB_OK ||
+  void *d_desc, *d_wl, *d_coff, *d_cone, *d_lmask, *d_fail, *d_maxp, *d_psum, *d_minp = nullptr;
+  if ((st = ws_buffer(c, ws, tmp, 0, count * sizeof(WinDesc6), &d_desc)) != GB_OK ||
+      (st = ws_buffer(c, ws, tmp, 1, count * sizeof(WinLarge), &d_wl)) != GB_OK ||
       (st = ws_buffer(c, ws, tmp, 2, (count + 1) * 8, &d_coff)) != GB_OK ||
-      (st = ws_buffer(c, ws, tmp, 3, words * 4, &d_bits)) != GB_OK ||
-      (st = ws_buffer(c, ws, tmp, 4, count * 4, &d_fail)) != GB_OK ||
-      (st = ws_buffer(c, ws, tmp, 5, count * 8, &d_maxp)) != GB_OK ||
-      (st = ws_buffer(c, ws, tmp, 6, count * 8, &d_psum)) != GB_OK ||
-      (min_p_concat && (st = ws_buffer(c, ws, tmp, 7, total_n * 4, &d_minp)) != GB_OK))
+      (st = ws_buffer(c, ws, tmp, 3, 2 * count * 8, &d_cone)) != GB_OK ||
+      (st = ws_buffer(c, ws, tmp, 4, lwords_total * 4, &d_lmask)) != GB_OK ||
+      (st = ws_buffer(c, ws, tmp, 5, count * 4, &d_fail)) != GB_OK ||
+      (st = ws_buffer(c, ws, tmp, 6, count * 8, &d_maxp)) != GB_OK ||
+      (st = ws_buffer(c, ws, tmp, 7, count * 8, &d_psum)) != GB_OK ||
+      (min_p_concat && (st = ws_buffer(c, ws, tmp, 8, total_n * 4, &d_minp)) != GB_OK))
     return st;
-  WindowsArgs a{};
+
+  RangeArgs a{};
   SearchParams& sp = a.s;
   sp.halo = H;
   sp.nsearch = (uint32_t)ns;
-  sp.klock = (uint32_t)std::min<uint64_t>(ns, kLockPrimes);
   sp.kfb = (uint32_t)std::min<uint64_t>(kf, 0xffffffffu);
   sp.p_lim = p_lim;
   sp.p_small = p_lim;
@@ -126,60 +139,98 @@ static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, cons
   sp.minp = (uint32_t*)d_minp;
   sp.queue = ws.queue;
   sp.queue_cap = ws.queue_cap;
-  a.win = (const WinDesc*)d_desc;
-  a.wg = (const longlong2*)((char*)d_desc + desc_bytes);
-  a.nwin = (uint32_t)count;
-  a.tile_off = (const uint64_t*)d_toff;
-  a.chunk_off = (const uint64_t*)d_coff;
-  a.total_tiles = tile_off[count];
-  a.total_chunks = chunk_off[count];
-  a.tile_bits = kWinTileBits;
   a.chunk_evens = NE;
-  a.nbw = (H / 2 + NE + 64) / 32 + 8;
-  a.bits = (uint32_t*)d_bits;
+  a.nbw = nbw;
   a.magic = c->d_magic;
-  a.nsmall = (uint32_t)std::max<uint64_t>(nsmall, kWheelPrimeCount + 1);
+  a.nsieve = (uint32_t)std::max<uint64_t>(nsmall, kWheelPrimeCount + 1);
   a.kcoop = (uint32_t)std::max<uint64_t>(std::min(kc, nsmall), kWheelPrimeCount + 1);
-  a.nlarge = (uint32_t)std::max<uint64_t>(nlarge, a.nsmall);
-  a.wheel = c->d_wheel;
+  a.wheel6 = c->d_wheel6;
+  a.a15 = c->d_a15;
+  a.win = (const WinDesc6*)d_desc;
+  a.chunk_off = (const uint64_t*)d_coff;
+  a.nwin = (uint32_t)count;
+  a.lmask = (const uint32_t*)d_lmask;
+  a.total_items = chunk_off[count];
+  WinLargeArgs la{};
+  la.win = (const WinDesc6*)d_desc;
+  la.wl = (const WinLarge*)d_wl;
+  la.w_lo = 0;
+  la.w_hi = (uint32_t)count;
+  la.primes = c->d_primes;
+  la.magic = c->d_magic;
+  la.a15 = c->d_a15;
+  la.k0 = (uint32_t)std::max<uint64_t>(nsmall, kWheelPrimeCount + 1);
+  la.k1 = (uint32_t)std::max<uint64_t>(nlarge, la.k0);
+  la.lmask = (uint32_t*)d_lmask;
+
+  const int sm = c->sm_count;
+  int bps = range_max_blocks_per_sm(a);
+  if (bps < 1) bps = 1;
+  const uint64_t grid_max = (uint64_t)sm * bps;
+  a.surv_cap = nbw;
+  {
+    void* p = nullptr;
+    if ((st = ws_scratch(c, ws, (size_t)grid_max * 6 * a.surv_cap * sizeof(uint2), &p)) != GB_OK) return st;
+    a.surv = (uint2*)p;
+  }
+  const uint64_t np = la.k1 - la.k0;
+  const int gl = (int)std::max<uint64_t>(1, std::min<uint64_t>((np + 255) / 256, (uint64_t)sm * kLargeBlocksPerSM));
 
   cudaStream_t s = o.stream ? (cudaStream_t)o.stream : c->stream;
   cudaError_t e = cudaSuccess;
   auto chk = [&](cudaError_t x) {
     if (e == cudaSuccess && x != cudaSuccess) e = x;
   };
-  chk(cudaMemcpyAsync(d_desc, desc.data(), count * sizeof(WinDesc), cudaMemcpyHostToDevice, s));
-  chk(cudaMemcpyAsync((void*)a.wg, wg.data(), count * sizeof(longlong2), cudaMemcpyHostToDevice, s));
-  chk(launch_win_nsieve((WinDesc*)d_desc, (uint32_t)count, c->d_primes, c->nprimes, s));
-  chk(cudaMemcpyAsync(d_toff, tile_off.data(), (count + 1) * 8, cudaMemcpyHostToDevice, s));
+  chk(cudaMemcpyAsync(d_desc, desc.data(), count * sizeof(WinDesc6), cudaMemcpyHostToDevice, s));
+  chk(cudaMemcpyAsync(d_wl, wl.data(), count * sizeof(WinLarge), cudaMemcpyHostToDevice, s));
   chk(cudaMemcpyAsync(d_coff, chunk_off.data(), (count + 1) * 8, cudaMemcpyHostToDevice, s));
+  chk(cudaMemcpyAsync(d_cone, chunk_one.data(), 2 * count * 8, cudaMemcpyHostToDevice, s));
   chk(cudaMemsetAsync(d_fail, 0, count * 4, s));
   chk(cudaMemsetAsync(d_maxp, 0, count * 8, s));
   chk(cudaMemsetAsync(d_psum, 0, count * 8, s));
   if (d_minp) chk(cudaMemsetAsync(d_minp, 0, total_n * 4, s));
   chk(cudaMemsetAsync(sp.ctr, 0, kCtrCount * 8, s));
   chk(cudaMemsetAsync(sp.ctr + kCtrFirstFail, 0xff, 8, s));
+  chk(launch_win_pairs((const WinDesc6*)d_desc, (uint32_t)count, c->d_primes, c->nprimes, la.k0,
+                       sp.ctr + kCtrWork2, s));
   chk(cudaStreamSynchronize(s));  // host vectors above are pageable and local
   int launches = 0;
-  const int sm = c->sm_count;
+  float large_ms = 0, search_ms = 0;
   chk(cudaEventRecord(ws.ev0, s));
   if (o.mode == GB_WINDOWS_PERSISTENT) {
-    const uint64_t np = a.nlarge - a.nsmall;
-    const int gl = (int)std::min<uint64_t>((np + 255) / 256, (uint64_t)sm * kLargeBlocksPerSM);
-    chk(launch_window_stages(a, 0xffffffffu, sm * 3, gl, sm * 2, s, &launches));
-    chk(launch_fallback(sp, sm * 4, s));
-    ++launches;
-  } else {
-    const uint64_t np = a.nlarge - a.nsmall;
-    const int gl = (int)std::min<uint64_t>((np + 255) / 256, (uint64_t)sm * kLargeBlocksPerSM);
-    for (uint32_t r = 0; r < count && e == cudaSuccess; ++r) {
-      const uint64_t nt = tile_off[r + 1] - tile_off[r];
-      const uint64_t nc = chunk_off[r + 1] - chunk_off[r];
-      chk(cudaMemsetAsync(sp.ctr + kCtrQueue, 0, 8, s));
-      chk(launch_window_stages(a, r, (int)std::min<uint64_t>(nt, sm * 3), gl,
-                               (int)std::min<uint64_t>(nc, sm * 2), s, &launches));
-      chk(launch_fallback(sp, std::max(1, sm / 4), s));
+    chk(cudaMemsetAsync(d_lmask, 0xff, lwords_total * 4, s));
+    chk(cudaEventRecord(ws.ek0, s));
+    if (la.k1 > la.k0) {
+      chk(launch_win_large(la, gl, s));
       ++launches;
+    }
+    chk(cudaEventRecord(ws.ek1, s));
+    const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(grid_max, a.total_items));
+    chk(launch_range(a, grid, s));
+    chk(cudaEventRecord(ws.ek2, s));
+    chk(launch_fallback(sp, sm * 4, s));
+    launches += 2;
+  } else {
+    for (uint32_t r = 0; r < count && e == cudaSuccess; ++r) {
+      const WinDesc6& d = desc[r];
+      chk(cudaMemsetAsync((uint32_t*)d_lmask + d.lbase, 0xff, 2ull * d.lwords * 4, s));
+      chk(cudaMemsetAsync(sp.ctr + kCtrWork, 0, 8, s));
+      chk(cudaMemsetAsync(sp.ctr + kCtrQueue, 0, 8, s));
+      WinLargeArgs l1 = la;
+      l1.w_lo = r;
+      l1.w_hi = r + 1;
+      if (l1.k1 > l1.k0 && d.q_top >= kWinChunkSieveBound * kWinChunkSieveBound) {
+        chk(launch_win_large(l1, gl, s));
+        ++launches;
+      }
+      RangeArgs a1 = a;
+      a1.win = (const WinDesc6*)d_desc + r;
+      a1.chunk_off = (const uint64_t*)d_cone + 2 * r;
+      a1.nwin = 1;
+      a1.total_items = chunk_one[2 * r + 1];
+      chk(launch_range(a1, (int)std::min<uint64_t>(grid_max, a1.total_items), s));
+      chk(launch_fallback(sp, std::max(1, sm / 4), s));
+      launches += 2;
     }
   }
   chk(cudaEventRecord(ws.ev1, s));
@@ -193,7 +244,13 @@ static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, cons
   if (d_minp) chk(cudaMemcpyAsync(min_p_concat, d_minp, total_n * 4, cudaMemcpyDeviceToHost, s));
   chk(cudaStreamSynchronize(s));
   float ms = 0;
-  if (e == cudaSuccess) cudaEventElapsedTime(&ms, ws.ev0, ws.ev1);
+  if (e == cudaSuccess) {
+    cudaEventElapsedTime(&ms, ws.ev0, ws.ev1);
+    if (o.mode == GB_WINDOWS_PERSISTENT) {
+      cudaEventElapsedTime(&large_ms, ws.ek0, ws.ek1);
+      cudaEventElapsedTime(&search_ms, ws.ek1, ws.ek2);
+    }
+  }
   if (e != cudaSuccess) return cuda_fail(ws, e, "windows");
   if (ctr[kCtrQueueOvf]) return fail(ws, GB_EOVERFLOW, "Phase-2 queue overflow: raise the halo");
   if (res) {
@@ -209,6 +266,10 @@ static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, cons
     sum->failures = ctr[kCtrFailures];
     sum->kernel_launches = launches;
     sum->device_ms = ms;
+    sum->sieved_windows = count;
+    sum->large_pairs = ctr[kCtrWork2];
+    sum->large_ms = large_ms;
+    sum->search_ms = search_ms;
   }
   return GB_OK;
 }
@@ -319,7 +380,7 @@ gb_status windows_impl(gb_ctx* c, Workspace& ws, Arena* arena, const gb_window* 
     uint64_t lim = o.mr_below;
     if (!lim) {
       const double r = std::sqrt((double)last);
-      lim = r > 1e4 ? (uint64_t)(1.1 * r / std::log(r) / 2600.0) : 0;
+      lim = r > 1e4 ? (uint64_t)(1.1 * r / std::log(r) / kMrBelowDivisor) : 0;
     }
     narrow[i] = w[i].count < lim;
     nn += narrow[i];
@@ -327,7 +388,7 @@ gb_status windows_impl(gb_ctx* c, Workspace& ws, Arena* arena, const gb_window* 
   if (nn == 0) return windows_sieve_impl(c, ws, arena, w, count, opts, res, min_p_concat, sum);
   const uint64_t p_lim = o.phase2_limit ? o.phase2_limit : GB_PHASE2_LIMIT_DEFAULT;
   if (p_lim > GB_P_SMALL_MAX) return fail(ws, GB_EINVAL, "phase2_limit must be <= 4e9");
-  gb_status st = ensure_primes(c, ws, std::max<uint64_t>(p_lim, kWinSmallPrimeBound));
+  gb_status st = ensure_primes(c, ws, std::max<uint64_t>(p_lim, kWinChunkSieveBound));
   if (st != GB_OK) return st;
   // both parts in their own arrays, results put back in the caller's order
   std::vector<gb_window> wa, wb;
@@ -366,6 +427,10 @@ gb_status windows_impl(gb_ctx* c, Workspace& ws, Arena* arena, const gb_window* 
     sum->failures = sa.failures + sb.failures;
     sum->kernel_launches = sa.kernel_launches + sb.kernel_launches;
     sum->device_ms = sa.device_ms + sb.device_ms;
+    sum->sieved_windows = sb.sieved_windows;
+    sum->large_pairs = sb.large_pairs;
+    sum->large_ms = sb.large_ms;
+    sum->search_ms = sb.search_ms;
   }
   return GB_OK;
 }

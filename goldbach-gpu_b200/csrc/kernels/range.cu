@@ -20,10 +20,8 @@
 #include "../gb_device.cuh"
 #include "../gb_internal.h"
 #include "gb/gb.h"
-#include "search.cuh"
 #include "search6.cuh"
 #include "sieve6.cuh"
-#include "sieve_window.cuh"
 
 namespace gb {
 
@@ -41,10 +39,25 @@ __device__ __forceinline__ int64_t window_g0(uint64_t A, uint32_t H) {
   return -(int64_t)(((uint64_t)H + 1 - A + 5) / 6);
 }
 
+// last window w with off[w] <= item (off: nwin + 1 ascending prefix sums)
+__device__ __forceinline__ uint32_t find_item_window(const uint64_t* off, uint32_t nwin, uint64_t item) {
+  uint32_t lo = 0, hi = nwin;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (off[mid] <= item) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
 template <bool MINP>
 __global__ void __launch_bounds__(kRange6Threads, kRange6Blocks) range6_kernel(const __grid_constant__ RangeArgs a) {
   const SearchParams& s = a.s;
   __shared__ unsigned long long s_item;
+  // windows mode: the item's window and chunk, decoded by thread 0
+  __shared__ uint64_t s_wA, s_wbase, s_wunit, s_wlbase;
+  __shared__ int64_t s_wg0;
+  __shared__ uint32_t s_wcnt, s_wlwords;
   const int tid = threadIdx.x;
   Ctx6& cx = g_cx6;
   uint32_t* pat6 = smem6_pat();
@@ -63,6 +76,18 @@ __global__ void __launch_bounds__(kRange6Threads, kRange6Blocks) range6_kernel(c
   for (;;) {
     if (tid == 0) {
       s_item = atomicAdd(&s.ctr[kCtrWork], 1ull);
+      if (a.win && s_item < a.total_items) {
+        const uint32_t w = find_item_window(a.chunk_off, a.nwin, s_item);
+        const WinDesc6 d = a.win[w];
+        const uint64_t j0 = (s_item - a.chunk_off[w]) * a.chunk_evens;
+        s_wA = d.start + 2 * j0;
+        s_wcnt = (uint32_t)(d.count - j0 < a.chunk_evens ? d.count - j0 : a.chunk_evens);
+        s_wbase = d.out_off + j0;
+        s_wunit = d.orig;
+        s_wg0 = d.g0;
+        s_wlbase = d.lbase;
+        s_wlwords = d.lwords;
+      }
       cx.fb = 0;
       cx.maxp = 0;
       cx.psum = 0;
@@ -76,24 +101,35 @@ __global__ void __launch_bounds__(kRange6Threads, kRange6Blocks) range6_kernel(c
     __syncthreads();
     const unsigned long long item = s_item;
     if (item >= a.total_items) break;
-    const uint64_t ls = item / a.chunks_per_seg;
-    const uint64_t ci = item - ls * a.chunks_per_seg;
-    const uint64_t seg = a.shard_index + ls * a.shard_count;
-    const uint64_t seg_first = seg * a.seg_size;
-    const uint64_t seg_rem = a.total_count - seg_first;
-    const uint64_t seg_cnt = seg_rem < a.seg_size ? seg_rem : a.seg_size;
-    const uint64_t j0 = ci * a.chunk_evens;
-    if (j0 >= seg_cnt) {
-      __syncthreads();
-      continue;
+    uint64_t A, base_idx, unit;
+    uint32_t cnt;
+    if (a.win) {
+      A = s_wA;
+      cnt = s_wcnt;
+      base_idx = s_wbase;
+      unit = s_wunit;
+    } else {
+      const uint64_t ls = item / a.chunks_per_seg;
+      const uint64_t ci = item - ls * a.chunks_per_seg;
+      const uint64_t seg = a.shard_index + ls * a.shard_count;
+      const uint64_t seg_first = seg * a.seg_size;
+      const uint64_t seg_rem = a.total_count - seg_first;
+      const uint64_t seg_cnt = seg_rem < a.seg_size ? seg_rem : a.seg_size;
+      const uint64_t j0 = ci * a.chunk_evens;
+      if (j0 >= seg_cnt) {
+        __syncthreads();
+        continue;
+      }
+      A = a.start + 2 * (seg_first + j0);
+      cnt = (uint32_t)(seg_cnt - j0 < a.chunk_evens ? seg_cnt - j0 : a.chunk_evens);
+      base_idx = seg_first + j0;
+      unit = seg;
     }
-    const uint64_t A = a.start + 2 * (seg_first + j0);
-    const uint32_t cnt = (uint32_t)(seg_cnt - j0 < a.chunk_evens ? seg_cnt - j0 : a.chunk_evens);
     const int64_t G0 = window_g0(A, s.halo);
     if (tid == 0) {
       cx.A = A;
-      cx.base_idx = seg_first + j0;
-      cx.unit = seg;
+      cx.base_idx = base_idx;
+      cx.unit = unit;
       const uint64_t last = A + 2ull * (cnt - 1);
       const uint32_t amod = (uint32_t)(A % 6);
       // A - 6 G0 is in [H + 1, H + 7), so every X fits 32 bits
@@ -109,9 +145,21 @@ __global__ void __launch_bounds__(kRange6Threads, kRange6Blocks) range6_kernel(c
       }
     }
     const uint32_t nbits = s.halo / 6 + cnt / 3 + 96;
+    // words the search can read for a real n (a word past them only meets
+    // an empty unverified mask): a short chunk sieves no more than these
+    const uint32_t nwords = min(a.nbw, (nbits + 31) / 32 + 2);
+    const uint32_t* L1 = nullptr;
+    const uint32_t* L5 = nullptr;
+    uint32_t lsh = 0;
+    if (a.win) {  // the window's large-prime mask from this chunk's base on
+      const uint64_t d = (uint64_t)(G0 - s_wg0);
+      L1 = a.lmask + s_wlbase + (d >> 5);
+      L5 = L1 + s_wlwords;
+      lsh = (uint32_t)(d & 31);
+    }
     // q <= n - 3: the chunk's last n bounds the sieve (A + 2 cnt could pass 2^64)
-    sieve_window6<kRange6Threads>(Q1, Q5, a.nbw, nbits, G0, A + 2ull * (cnt - 1), pat6, s.primes,
-                                 a.magic, a.a15, a.nsieve, a.kcoop);
+    sieve_window6<kRange6Threads>(Q1, Q5, nwords, nbits, G0, A + 2ull * (cnt - 1), pat6, s.primes,
+                                 a.magic, a.a15, a.nsieve, a.kcoop, L1, L5, lsh);
     search_chunk6<MINP, kRange6Threads>(s);
   }
 }

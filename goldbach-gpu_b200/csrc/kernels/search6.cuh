@@ -1,7 +1,7 @@
 // search6.cuh -- word-parallel minimal-p search on the mod-6 layout.
 //
-// Same job as search.cuh (and as goldbach_phase1_kernel, src/goldbach.cu:
-// 288-311): the first prime p, ascending, with n - p prime.  The even n of
+// Same job as goldbach_phase1_kernel (src/goldbach.cu:288-311): the first
+// prime p, ascending, with n - p prime.  The even n of
 // a chunk are split by n mod 6 = rho in {0, 2, 4}; a U word holds 32 n of
 // one class, bit m <-> n = n_rho + 6m.  q = n - p must avoid 0 (mod 3), so
 //   rho = 2: p = 3 (q in class 5), then primes p = 1 (mod 6) (q in class 1);
@@ -30,9 +30,10 @@
 #include "../gb_device.cuh"
 #include "../gb_internal.h"
 #include "gb/gb.h"
-#include "search.cuh"
 
 namespace gb {
+
+constexpr int kSmemHistBins = 1024;  // per-CTA minimal-p histogram bins in shared memory
 
 constexpr uint32_t kE6UBits = 15;
 constexpr uint32_t kLockSteps6 = 128; // lockstep entries of each class sequence
@@ -65,7 +66,7 @@ struct Ctx6 {
   // the chunk
   uint64_t A;         // first even n
   uint64_t base_idx;  // output index of n = A
-  uint64_t unit;      // segment
+  uint64_t unit;      // segment (range) or caller's window index (windows)
   uint64_t n[3];      // n_rho: first n of each class
   uint32_t M[3];      // n of each class
   uint32_t K[3][2];   // K for q-class 1 and 5
@@ -382,8 +383,8 @@ __device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_
   }
 }
 
-// Whole-chunk search by the CTA plus the flush of its accounting (same
-// contract as search_chunk in search.cuh).  The histogram, g_cx6's fb,
+// Whole-chunk search by the CTA plus the flush of its accounting into the
+// call's counters and the chunk's unit.  The histogram, g_cx6's fb,
 // maxp, psum, maxk, scnt and next_task must be zero before the call, and
 // g_cx6's survivor lists set (surv_cap >= words of a class).  Warps take
 // each level's tasks from a shared counter, classes 2 and 4 first.  Ends

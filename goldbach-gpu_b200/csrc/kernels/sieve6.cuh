@@ -62,15 +62,20 @@ __device__ __forceinline__ uint32_t base_mod(int64_t G0, uint32_t p, uint64_t ma
 // Sieves bits [0, nbits) of both class bitsets (nwords words each written).
 // Exact for every q <= q_top.  pat6: the class wheel patterns (shared
 // memory).  primes[kWheelPrimeCount+1 .. nsieve) are the marking primes
-// (71, 73, ...), those below kcoop marked warp-cooperatively.  Ends with
-// __syncthreads().
+// (71, 73, ...), those below kcoop marked warp-cooperatively.  With a mask
+// (L1 non-null), word t of each class is also ANDed with the 32 mask bits
+// from bit lsh of word t of L1 / L5 (the multiples of the primes beyond
+// nsieve, cleared by the windows' large-prime pass); the mask must hold
+// nwords + 1 words from there.  Ends with __syncthreads().
 template <int NT>
 __device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ Q5,
                               uint32_t nwords, uint32_t nbits, int64_t G0, uint64_t q_top,
                               const uint32_t* __restrict__ pat6,
                               const uint32_t* __restrict__ primes,
                               const uint64_t* __restrict__ magic, const uint2* __restrict__ a15,
-                              uint32_t nsieve, uint32_t kcoop) {
+                              uint32_t nsieve, uint32_t kcoop,
+                              const uint32_t* __restrict__ L1 = nullptr,
+                              const uint32_t* __restrict__ L5 = nullptr, uint32_t lsh = 0) {
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
@@ -100,6 +105,10 @@ __device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ 
         w &= __funnelshift_r(pp[0], pp[1], rr & 31);
         const uint32_t nr = rr + step;
         r[x] = nr >= P ? nr - P : nr;
+      }
+      if (L1) {
+        const uint32_t* L = cls5 ? L5 : L1;
+        w &= __funnelshift_r(__ldg(L + t), __ldg(L + t + 1), lsh);
       }
       Q[t] = w;
     }

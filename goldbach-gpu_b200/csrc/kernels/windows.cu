@@ -1,28 +1,39 @@
-// windows.cu -- batched verification of many independent windows of even n.
+// windows.cu -- batched verification of many independent windows of even n:
+// the large-prime pass, and the expansion of narrow windows for the
+// Miller-Rabin path.
 //
 // The reference verifies one contiguous range at a time with a host loop of
 // launches per segment (src/goldbach.cu:420-485).  Windows far out (starts
-// up to 1e18) need sieving primes up to 1e9, where recomputing every prime's
-// first multiple per CTA chunk (as the fused range kernel does for primes up
-// to 1e6) would cost ~5e7 divisions per chunk.  The batch is therefore
-// staged through HBM:
-//   A. tile sieve: every window's odd q-bitset [start-H+1, end] is sieved
-//      tile by tile in shared memory with the wheel and the primes < 2^17,
-//      and stored with coalesced 128-bit stores;
-//   B. large primes: one thread per prime p in [2^17, sqrt(max q)] walks the
-//      windows (sorted by their top q, so only those with p^2 <= top are
-//      visited), computes the first multiple from a double-precision
-//      quotient estimate (one remainder per window: the stage's whole cost)
-//      and clears its multiples with global atomicAnd (at most a few per
-//      window);
-//   C. search: every chunk of NE even n loads its q-window from HBM into
-//      shared memory and runs the same word-parallel search as the range
-//      kernel (search.cuh);
-//   D. the device Phase 2 (range.cu fallback_kernel) for minimal p >= H.
-// In the persistent mode each stage is ONE launch over the whole batch, its
-// CTAs pulling items from a device work counter.  In the plain mode the same
-// four stages run window by window (the per-window launch pipeline), for
-// comparison.
+// up to 1e18) need sieving primes up to 1e9, and every one of those primes
+// needs its first multiple in every window: about 1e11 (prime, window)
+// pairs for the 4096 seeded windows in [1e15, 1e18], of which only a few
+// percent have a multiple in the window at all.  The batch is therefore
+// split by prime size:
+//   1. this pass: one thread per prime p above the chunk sieve's bound walks
+//      the windows (sorted by their top, so only those with p^2 <= top are
+//      visited) and clears p's multiples in each window's two class masks
+//      (mod-6 layout, bit t <-> q = 6(g0 + t) + c, c in {1, 5}) with global
+//      atomicAnd;
+//   2. range6_kernel in windows mode: every (window, chunk) item sieves its
+//      q-window in shared memory with the wheel and the primes up to the
+//      bound, ANDs in the window's masks, and runs the levelled search;
+//   3. the device Phase 2 (range.cu fallback_kernel) for minimal p beyond
+//      the halo.
+//
+// Cost of a pair.  With r = g0 mod p, the first marks of the two classes
+// are t_c = (a_c - r) mod p (a_1 = -1/6, a_5 = -5/6 mod p, from the a15
+// table).  r comes from a double-precision quotient estimate: g0 < 2^62 and
+// p > 2^20, so the fused multiply-add of the window's g0 (as a double) by
+// 1/p, added to 1.5 * 2^52, rounds to round(g0 / p) with an error far below
+// 1/2 -- floor(g0 / p) or one more -- and the low 32 bits of that double are
+// round(g0 / p) mod 2^32.  r = low32(g0) - p * round(g0 / p) (mod 2^32) then
+// lies in (-p, p), so 32-bit arithmetic finishes it (p < 2^31).  One 16-byte
+// record per window holds g0 as a double, its low 32 bits and the mask
+// length; the descriptor is read only on a hit.  The pass marks every
+// multiple of p in the window, those below p^2 included (they are
+// composite); only p itself must stay, and it can lie in a window only when
+// the window starts below 2^32, so those windows (g0 < 2^30) take an exact
+// path with the p^2 rule.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -30,172 +41,111 @@
 #include "../gb_device.cuh"
 #include "../gb_internal.h"
 #include "gb/gb.h"
-#include "search.cuh"
-#include "sieve_window.cuh"
+#include "sieve6.cuh"
 
 namespace gb {
 
-constexpr int kWinThreads = 512;
+constexpr int kWinLargeThreads = 256;
 
-__device__ __forceinline__ uint32_t find_window(const uint64_t* off, uint32_t nwin, uint64_t item) {
-  uint32_t lo = 0, hi = nwin;  // last w with off[w] <= item
-  while (hi - lo > 1) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (off[mid] <= item) lo = mid;
-    else hi = mid;
-  }
-  return lo;
+// Exact marks of p in window w: first marks from the signed base with the
+// p^2 rule (sieve6.cuh), then every p-th bit of both class masks.
+__device__ __noinline__ void win_mark_exact(const WinLargeArgs& a, uint32_t w, uint32_t p, uint32_t k) {
+  const WinDesc6 d = a.win[w];
+  const uint32_t lbits = d.lwords * 32;
+  uint32_t t1, t5;
+  first_marks6(d.g0, p, __ldg(a.a15 + k), base_mod(d.g0, p, __ldg(a.magic + k)), lbits, t1, t5);
+  uint32_t* L1 = a.lmask + d.lbase;
+  uint32_t* L5 = L1 + d.lwords;
+  for (uint64_t i = t1; i < lbits; i += p) atomicAnd(&L1[i >> 5], ~(1u << (i & 31)));
+  for (uint64_t i = t5; i < lbits; i += p) atomicAnd(&L5[i >> 5], ~(1u << (i & 31)));
 }
 
-// Per-window sieving bound: nsieve = #primes <= isqrt(q_top) (binary search
-// in the resident table), so the host never looks these up one by one.
-__global__ void win_nsieve_kernel(WinDesc* win, uint32_t nwin, const uint32_t* primes,
-                                  uint64_t nprimes) {
-  const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
-  if (w >= nwin) return;
-  const uint64_t q = win[w].q_top;
-  uint64_t r = (uint64_t)sqrt((double)q);
-  while (r > 0 && (r > 0xffffffffull || r * r > q)) --r;
-  while (r < 0xffffffffull && (r + 1) * (r + 1) <= q) ++r;
-  uint64_t lo = 0, hi = nprimes;  // first index with primes[i] > r
-  while (lo < hi) {
-    const uint64_t mid = (lo + hi) >> 1;
-    if (primes[mid] <= r) lo = mid + 1;
-    else hi = mid;
-  }
-  win[w].nsieve = (uint32_t)(lo > kWheelPrimeCount + 1 ? lo : kWheelPrimeCount + 1);
+// Marks from the fast path's first marks t1, t5 (< p < 2^31) up to lbits.
+__device__ __noinline__ void win_mark_from(const WinLargeArgs& a, uint32_t w, uint32_t p, uint32_t t1,
+                                           uint32_t t5, uint32_t lbits) {
+  const uint64_t lbase = a.win[w].lbase;
+  const uint32_t lwords = a.win[w].lwords;
+  uint32_t* L1 = a.lmask + lbase;
+  uint32_t* L5 = L1 + lwords;
+  for (uint32_t i = t1; i < lbits; i += p) atomicAnd(&L1[i >> 5], ~(1u << (i & 31)));
+  for (uint32_t i = t5; i < lbits; i += p) atomicAnd(&L5[i >> 5], ~(1u << (i & 31)));
 }
 
-cudaError_t launch_win_nsieve(WinDesc* win, uint32_t nwin, const uint32_t* primes, uint64_t nprimes,
-                              cudaStream_t s) {
-  if (!nwin) return cudaSuccess;
-  win_nsieve_kernel<<<(nwin + 255) / 256, 256, 0, s>>>(win, nwin, primes, nprimes);
+__global__ void __launch_bounds__(kWinLargeThreads) win_large_kernel(const __grid_constant__ WinLargeArgs a) {
+  const uint32_t stride = gridDim.x * kWinLargeThreads;
+  for (uint32_t k = a.k0 + blockIdx.x * kWinLargeThreads + threadIdx.x; k < a.k1; k += stride) {
+    const uint32_t p = __ldg(a.primes + k);
+    const uint64_t pp = (uint64_t)p * p;
+    // first window whose top reaches p^2 (windows sorted by q_top)
+    uint32_t lo = a.w_lo, hi = a.w_hi;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (a.win[mid].q_top < pp) lo = mid + 1;
+      else hi = mid;
+    }
+    if (p >= 0x80000000u) {  // windows near 2^64 only: every pair exact
+      for (uint32_t w = lo; w < a.w_hi; ++w) win_mark_exact(a, w, p, k);
+      continue;
+    }
+    const double inv = 1.0 / (double)p;
+    const uint2 ac = __ldg(a.a15 + k);
+    const uint32_t a1 = ac.x;
+    const uint32_t dl = ac.y >= ac.x ? ac.y - ac.x : ac.y + p - ac.x;  // a5 - a1 mod p
+    const double kRound = 6755399441055744.0;                         // 1.5 * 2^52
+#pragma unroll 4
+    for (uint32_t w = lo; w < a.w_hi; ++w) {
+      const WinLarge v = a.wl[w];
+      const uint32_t qe = (uint32_t)__double_as_longlong(fma(v.gd, inv, kRound));
+      uint32_t r = v.gl - qe * p;  // g0 - p round(g0 / p), in (-p, p)
+      r = min(r, r + p);           // [0, p)
+      uint32_t t1 = a1 - r;
+      t1 = min(t1, t1 + p);
+      uint32_t t5 = t1 + dl;
+      t5 = min(t5, t5 - p);
+      if (min(t1, t5) < v.lbits) {  // a mark in the window, or the exact path
+        if (v.lbits == 0xffffffffu) win_mark_exact(a, w, p, k);
+        else win_mark_from(a, w, p, t1, t5, v.lbits);
+      }
+    }
+  }
+}
+
+cudaError_t launch_win_large(const WinLargeArgs& a, int grid, cudaStream_t s) {
+  if (a.k1 <= a.k0 || a.w_hi <= a.w_lo || grid < 1) return cudaSuccess;
+  win_large_kernel<<<grid, kWinLargeThreads, 0, s>>>(a);
   return cudaGetLastError();
 }
 
-// A. tile sieve ---------------------------------------------------------------
-__global__ void __launch_bounds__(kWinThreads) win_tile_kernel(const __grid_constant__ WindowsArgs a,
-                                                               uint32_t w_only) {
-  extern __shared__ uint32_t smem[];
-  uint32_t* pat = smem;
-  uint32_t* Q = smem + kWheelWords;
-  __shared__ unsigned long long s_item;
-  for (uint32_t i = threadIdx.x; i < kWheelWords; i += kWinThreads) pat[i] = a.wheel[i];
-  const uint64_t lo_item = w_only < a.nwin ? a.tile_off[w_only] : 0;
-  const uint64_t hi_item = w_only < a.nwin ? a.tile_off[w_only + 1] : a.total_tiles;
-  for (;;) {
-    if (threadIdx.x == 0) s_item = lo_item + atomicAdd(&a.s.ctr[kCtrWork], 1ull);
-    __syncthreads();
-    const uint64_t item = s_item;
-    if (item >= hi_item) break;
-    const uint32_t w = w_only < a.nwin ? w_only : find_window(a.tile_off, a.nwin, item);
-    const WinDesc d = a.win[w];
-    const uint64_t t = item - a.tile_off[w];
-    const uint64_t b0 = t * a.tile_bits;
-    const uint32_t nb = (uint32_t)(d.wbits - b0 < a.tile_bits ? d.wbits - b0 : a.tile_bits);
-    const uint32_t nw = nb / 32;  // wbits and tile_bits are multiples of 32
-    const int64_t g0 = (int64_t)(d.start >> 1) - (int64_t)(a.s.halo >> 1) + (int64_t)b0;
-    // the tile's top q, or the window's when that is lower (compared in odd
-    // index space: the tile's top may pass 2^64 for windows ending near it)
-    const uint64_t gt = (uint64_t)(g0 + nb - 1);
-    const uint64_t q_top = gt >= (d.q_top >> 1) ? d.q_top : 2 * gt + 1;
-    const uint32_t ns = d.nsieve < a.nsmall ? d.nsieve : a.nsmall;
-    sieve_window<kWinThreads>(Q, nw, nb, g0, q_top, pat, a.s.primes, a.magic, ns, a.kcoop);
-    // 128-bit coalesced stores: wbase, b0 / 32 and nw are multiples of 4 words
-    uint4* out = reinterpret_cast<uint4*>(a.bits + d.wbase + b0 / 32);
-    for (uint32_t i = threadIdx.x; i < nw / 4; i += kWinThreads)
-      out[i] = make_uint4(Q[4 * i], Q[4 * i + 1], Q[4 * i + 2], Q[4 * i + 3]);
-    __syncthreads();
+// (prime, window) pairs the large-prime pass visits: for each window the
+// primes in [k0, pi(isqrt(q_top))), summed into *pairs.
+__global__ void win_pairs_kernel(const WinDesc6* __restrict__ win, uint32_t nwin,
+                                 const uint32_t* __restrict__ primes, uint64_t nprimes, uint32_t k0,
+                                 unsigned long long* pairs) {
+  const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w < nwin) {
+    const uint64_t q = win[w].q_top;
+    uint64_t r = (uint64_t)sqrt((double)q);
+    while (r > 0 && (r > 0xffffffffull || r * r > q)) --r;
+    while (r < 0xffffffffull && (r + 1) * (r + 1) <= q) ++r;
+    uint64_t lo = 0, hi = nprimes;  // first index with primes[i] > r
+    while (lo < hi) {
+      const uint64_t mid = (lo + hi) >> 1;
+      if (primes[mid] <= r) lo = mid + 1;
+      else hi = mid;
+    }
+    if (lo > k0) atomicAdd(pairs, (unsigned long long)(lo - k0));
   }
 }
 
-// B. large primes -------------------------------------------------------------
-__global__ void __launch_bounds__(256) win_large_kernel(const __grid_constant__ WindowsArgs a,
-                                                        uint32_t w_only) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t k = a.nsmall + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < a.nlarge;
-       k += stride) {
-    const uint32_t p = a.s.primes[k];
-    const double inv = 1.0 / (double)p;  // p >= 2^17: first_mark_f64 applies
-    const uint64_t pp = (uint64_t)p * p;
-    const uint64_t gpp = (pp - 1) >> 1;
-    uint32_t w0, w1;
-    if (w_only < a.nwin) {
-      w0 = w_only;
-      w1 = w_only + 1;
-      if (a.win[w0].q_top < pp) continue;
-    } else {
-      // first window whose top reaches p^2 (windows sorted by q_top)
-      uint32_t lo = 0, hi = a.nwin;
-      while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (a.win[mid].q_top < pp) lo = mid + 1;
-        else hi = mid;
-      }
-      w0 = lo;
-      w1 = a.nwin;
-    }
-    // one 16-byte load per window; the descriptor only on a hit (p is at
-    // least 2^17, the bitsets 2^13..2^25 bits: most windows get none)
-#pragma unroll 8
-    for (uint32_t w = w0; w < w1; ++w) {
-      const longlong2 v = a.wg[w];
-      const uint64_t f = first_mark_f64(v.x, p, inv, gpp);
-      if (f < (uint64_t)v.y) {
-        uint32_t* bw = a.bits + a.win[w].wbase;
-        for (uint64_t i = f; i < (uint64_t)v.y; i += p) atomicAnd(&bw[i >> 5], ~(1u << (i & 31)));
-      }
-    }
-  }
+cudaError_t launch_win_pairs(const WinDesc6* win, uint32_t nwin, const uint32_t* primes, uint64_t nprimes,
+                             uint32_t k0, unsigned long long* pairs, cudaStream_t s) {
+  if (!nwin) return cudaSuccess;
+  win_pairs_kernel<<<(nwin + 255) / 256, 256, 0, s>>>(win, nwin, primes, nprimes, k0, pairs);
+  return cudaGetLastError();
 }
 
-// C. search -------------------------------------------------------------------
-template <bool MINP>
-__global__ void __launch_bounds__(kWinThreads, 2) win_search_kernel(const __grid_constant__ WindowsArgs a,
-                                                                    uint32_t w_only) {
-  extern __shared__ uint32_t smem[];
-  uint32_t* Q = smem;
-  uint32_t* HIST = Q + a.nbw;
-  uint16_t* SOFF = reinterpret_cast<uint16_t*>(HIST + kSmemHistBins);
-  __shared__ unsigned long long s_item, s_psum;
-  __shared__ uint32_t s_fb, s_maxp;
-  const SearchParams& s = a.s;
-  load_search_offsets<kWinThreads>(s, SOFF);
-  const uint64_t lo_item = w_only < a.nwin ? a.chunk_off[w_only] : 0;
-  const uint64_t hi_item = w_only < a.nwin ? a.chunk_off[w_only + 1] : a.total_chunks;
-  for (;;) {
-    if (threadIdx.x == 0) {
-      s_item = lo_item + atomicAdd(&s.ctr[kCtrWork2], 1ull);
-      s_fb = 0;
-      s_maxp = 0;
-      s_psum = 0;
-    }
-    for (uint32_t i = threadIdx.x; i < kSmemHistBins; i += kWinThreads) HIST[i] = 0;
-    __syncthreads();
-    const uint64_t item = s_item;
-    if (item >= hi_item) break;
-    const uint32_t w = w_only < a.nwin ? w_only : find_window(a.chunk_off, a.nwin, item);
-    const WinDesc d = a.win[w];
-    const uint64_t ci = item - a.chunk_off[w];
-    const uint64_t j0 = ci * a.chunk_evens;
-    Chunk c;
-    c.cnt = (uint32_t)(d.count - j0 < a.chunk_evens ? d.count - j0 : a.chunk_evens);
-    c.A = d.start + 2 * j0;
-    c.base_idx = d.out_off + j0;
-    c.unit = d.orig;  // caller's window index
-    // chunk window = bits [j0, j0 + H/2 + cnt + 64) of the window bitset
-    const uint32_t nwq = (s.halo / 2 + c.cnt + 64) / 32;
-    const uint4* src = reinterpret_cast<const uint4*>(a.bits + d.wbase + j0 / 32);
-    uint4* dst = reinterpret_cast<uint4*>(Q);
-    const uint32_t n4 = (nwq + 3) / 4;
-    for (uint32_t i = threadIdx.x; i < n4; i += kWinThreads) dst[i] = src[i];
-    __syncthreads();
-    search_chunk<MINP, kWinThreads>(s, Q, SOFF, HIST, c, &s_fb, &s_maxp, &s_psum);
-  }
-}
-
-// D. narrow windows on the Miller-Rabin path: the n of each window, laid out
-// window after window at off[i], for the single-n kernel -------------------
+// Narrow windows on the Miller-Rabin path: the n of each window, laid out
+// window after window at off[i], for the single-n kernel.
 __global__ void win_expand_kernel(const gb_window* __restrict__ w, const uint64_t* __restrict__ off,
                                   uint32_t nw, uint64_t* __restrict__ n) {
   for (uint32_t i = blockIdx.x; i < nw; i += gridDim.x) {
@@ -209,45 +159,6 @@ cudaError_t launch_win_expand(const gb_window* w, const uint64_t* off, uint32_t 
   if (!nw) return cudaSuccess;
   win_expand_kernel<<<nw < 4096 ? nw : 4096, 256, 0, s>>>(w, off, nw, n);
   return cudaGetLastError();
-}
-
-// ---------------------------------------------------------------------------
-static size_t tile_smem(const WindowsArgs& a) {
-  return (size_t)(kWheelWords + a.tile_bits / 32 + 2) * sizeof(uint32_t);
-}
-static size_t search_smem(const WindowsArgs& a) {
-  return (size_t)(a.nbw + kSmemHistBins) * sizeof(uint32_t) +
-         (size_t)((a.s.nsearch + 1) & ~1u) * sizeof(uint16_t);
-}
-
-cudaError_t launch_window_stages(const WindowsArgs& a, uint32_t w_only, int grid_tile,
-                                 int grid_large, int grid_search, cudaStream_t st, int* launches) {
-  cudaError_t e;
-  const size_t ts = tile_smem(a), ss = search_smem(a);
-  e = cudaFuncSetAttribute(win_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ts);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(win_search_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)ss);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(win_search_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)ss);
-  if (e != cudaSuccess) return e;
-  // the stages' work counters restart at 0
-  if ((e = cudaMemsetAsync(&a.s.ctr[kCtrWork], 0, 8, st)) != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(&a.s.ctr[kCtrWork2], 0, 8, st)) != cudaSuccess) return e;
-  win_tile_kernel<<<grid_tile, kWinThreads, ts, st>>>(a, w_only);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  ++*launches;
-  if (a.nlarge > a.nsmall && grid_large > 0) {
-    win_large_kernel<<<grid_large, 256, 0, st>>>(a, w_only);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    ++*launches;
-  }
-  if (a.s.minp) win_search_kernel<true><<<grid_search, kWinThreads, ss, st>>>(a, w_only);
-  else win_search_kernel<false><<<grid_search, kWinThreads, ss, st>>>(a, w_only);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  ++*launches;
-  return cudaSuccess;
 }
 
 }  // namespace gb

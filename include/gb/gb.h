@@ -260,9 +260,10 @@ gb_status gb_check_single_batch_noalloc(const uint64_t* n, size_t count, uint64_
  * Batched windows: many independent ranges of consecutive even n.
  * ---------------------------------------------------------------------- */
 typedef struct gb_window {
-  uint64_t start; /* first even n (>= 4)      */
-  uint64_t count; /* number of even n (>= 1)  */
+  uint64_t start; /* first even n (>= 4)                        */
+  uint64_t count; /* number of even n (1 .. GB_WINDOW_MAX_COUNT) */
 } gb_window;
+#define GB_WINDOW_MAX_COUNT (1ull << 33) /* wider ranges: gb_verify_range */
 
 #define GB_WINDOWS_PERSISTENT 0 /* one persistent launch, device work queue */
 #define GB_WINDOWS_PLAIN 1      /* one pipeline of launches per window      */
@@ -293,6 +294,10 @@ typedef struct gb_windows_summary {
   uint64_t failures;
   uint64_t kernel_launches;
   double device_ms;
+  uint64_t sieved_windows; /* windows on the sieve path (the rest: Miller-Rabin)  */
+  uint64_t large_pairs;    /* (prime, window) pairs of the large-prime pass       */
+  double large_ms;         /* device time of the large-prime pass (persistent)    */
+  double search_ms;        /* device time of the chunk sieve + search (persistent) */
 } gb_windows_summary;
 
 /* min_p_concat (nullable) receives the minimal p of every n, window after

@@ -107,7 +107,7 @@ def test_c3_sieve_and_miller_rabin_paths_on_wide_windows(ctx, c3_windows, mr_bel
     the Miller-Rabin path: the same minimal p."""
     s, c, want = c3_windows
     keep = c <= (1 << 21)
-    offs = np.concatenate([[0], np.cumsum(c)])
+    offs = np.concatenate([[0], np.cumsum(c.astype(np.int64))])
     sub = np.concatenate([want[offs[i]:offs[i + 1]] for i in np.nonzero(keep)[0]])
     _, minp, _ = ctx.verify_windows(s[keep], c[keep], want_minp=True, mr_below=mr_below)
     np.testing.assert_array_equal(minp, sub)
