@@ -67,6 +67,43 @@ def sieving_primes(limit):
     return sum(sieve)
 
 
+def search_floor(ctx, limit, strata=32, width=1 << 16):
+    """The word-parallel floor of the range search, from the kernel's own
+    per-n minimal p on `strata` seeded slices of `width` even n spread over
+    [4, limit]: the even n of a class rho = n mod 6 are searched 32 to a word
+    against the class's candidate sequence (rho 0: every prime >= 5; rho 2:
+    3, then the primes = 1 mod 6; rho 4: 3, then the primes = 5 mod 6), and
+    a word is done after the entries of its slowest n.  Returns (mean
+    sum-of-pi(p_min) tests per n, floor word-steps per n)."""
+    import numpy as np
+    top = 1 << 20
+    primes = ctx.primes_upto(top).astype(np.int64)
+    k0 = np.arange(len(primes), dtype=np.int64)
+    pi = np.zeros(top + 1, np.int64)  # prime -> its index (2 -> 0)
+    pi[primes] = k0
+    entry = {0: np.zeros(top + 1, np.int64)}  # prime -> entry index in the class sequence
+    entry[0][primes[2:]] = k0[2:] - 2
+    for rho, resid in ((2, 1), (4, 5)):
+        sel = primes[primes % 6 == resid]
+        entry[rho] = np.zeros(top + 1, np.int64)
+        entry[rho][sel] = np.arange(1, len(sel) + 1)
+    rng = np.random.default_rng(0xB200)
+    tests = steps = count = 0
+    for j in range(strata):
+        lo = 4 + (limit - 4 - 2 * width - (1 << 22)) * j // strata
+        a = lo - lo % 2 + 2 * int(rng.integers(0, 1 << 20))
+        r = ctx.verify_range(a, a + 2 * (width - 1), want_minp=True, want_hist=False)
+        mp = r.min_p.astype(np.int64)
+        n = a + 2 * np.arange(width, dtype=np.int64)
+        tests += int((pi[mp] + 1).sum())  # pi(p_min): the primes 2 .. p_min tried
+        for rho in (0, 2, 4):
+            e = entry[rho][mp[n % 6 == rho]] + 1
+            e = np.concatenate([e, np.zeros((-len(e)) % 32, np.int64)]).reshape(-1, 32)
+            steps += int(e.max(axis=1).sum())
+        count += width
+    return tests / count, steps / count
+
+
 def load_gb():
     spec = importlib.util.spec_from_file_location(
         "goldbach_gpu_b200", os.path.join(ROOT, "goldbach-gpu_b200", "__init__.py"))
@@ -206,19 +243,23 @@ def seeded_windows(seed=1, count=4096, lo=10**15, hi=10**18, wlo=10, whi=24):
     return starts, np.maximum(widths, 1)
 
 
-def measure_windows(gb, ctx):
+def measure_windows(gb, ctx, nwin=4096, plain=True):
     """C3: the whole batch in one persistent pipeline, and the plain
     per-window pipeline on the same 4096 windows; the per-window results of
-    the two must be identical."""
+    the two must be identical.  (nwin < 4096 and plain=False: the first nwin
+    seeded windows, persistent only -- a small case for profiling.)"""
     starts, counts = seeded_windows()
+    starts, counts = starts[:nwin], counts[:nwin]
     ctx.verify_windows(starts[:64], counts[:64])  # warm-up (tables to 1e9)
-    ctx.verify_windows(starts[:64], counts[:64], mode=gb.GB_WINDOWS_PLAIN)
+    if plain:
+        ctx.verify_windows(starts[:64], counts[:64], mode=gb.GB_WINDOWS_PLAIN)
     t0 = time.perf_counter()
     per, _, s = ctx.verify_windows(starts, counts, mode=gb.GB_WINDOWS_PERSISTENT)
     wall = time.perf_counter() - t0
     total = int(counts.sum())
     t1 = time.perf_counter()
-    per_p, _, sp = ctx.verify_windows(starts, counts, mode=gb.GB_WINDOWS_PLAIN)
+    per_p, _, sp = (ctx.verify_windows(starts, counts, mode=gb.GB_WINDOWS_PLAIN) if plain
+                    else (per, None, s))
     wall_p = time.perf_counter() - t1
     same = per == per_p
     pv = total / (sp["device_ms"] / 1e3)
@@ -456,6 +497,10 @@ def main():
     ap.add_argument("--ref-sample-log2", type=int, default=24)
     ap.add_argument("--extra", choices=["windows", "single", "counts", "serving"],
                     help="run only this secondary measurement and print its JSON (profiling)")
+    ap.add_argument("--windows", type=int, default=4096,
+                    help="--extra windows: the first N seeded windows only")
+    ap.add_argument("--no-windows-plain", action="store_true",
+                    help="--extra windows: skip the plain per-window pipeline")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -465,8 +510,11 @@ def main():
             print(json.dumps(measure_serving(gb, 0)))
         else:
             with gb.Context(0) as c:
-                f = {"windows": measure_windows, "single": measure_single, "counts": measure_counts}
-                print(json.dumps(f[args.extra](gb, c)))
+                if args.extra == "windows":
+                    print(json.dumps(measure_windows(gb, c, args.windows, not args.no_windows_plain)))
+                else:
+                    f = {"single": measure_single, "counts": measure_counts}
+                    print(json.dumps(f[args.extra](gb, c)))
         return 0
 
     import torch
@@ -587,6 +635,12 @@ def main():
     k_s = statistics.mean(kms) / 1000
     sol_s = alu_ops / alu_peak + marks / atom_peak
     achieved = (alu_ops + marks * alu_peak / atom_peak) / k_s
+    # the word-parallel floor: the search's SOL term counts one word op per 32
+    # (n, p) tests, but a word of 32 n runs until its slowest n is resolved
+    tests_per_n, floor_steps_per_n = search_floor(ctx, limit)
+    floor_ops = (alu_ops - n_mine * SEARCH_TESTS_PER_N / 32 * SEARCH_OPS_PER_WORD
+                 + n_mine * floor_steps_per_n * SEARCH_OPS_PER_WORD)
+    floor_s = floor_ops / alu_peak + marks / atom_peak
     hbm, hbm_kind = hbm_peak()
     hbm_bytes = 2 * n_mine * odd_q_per_n / 8  # the q-bitset, had it gone through HBM
     res0 = results[-1]
@@ -611,6 +665,14 @@ def main():
             "smem_atomic_peak": atom_peak, "alu_ops_per_launch": alu_ops,
             "smem_marks_per_launch": marks, "offsets_per_launch": offsets,
             "speed_of_light_ms": sol_s * 1e3,
+            "word_parallel_floor": {
+                "frac": floor_s / k_s, "floor_ms": floor_s * 1e3,
+                "floor_word_steps_per_n": floor_steps_per_n,
+                "sol_word_ops_per_n": SEARCH_TESTS_PER_N / 32,
+                "sampled_tests_per_n": tests_per_n,
+                "source": ("search term at the word-parallel floor (each word of 32 same-class n "
+                           "runs to its slowest n), from the kernel's per-n minimal p on 32 seeded "
+                           "slices of 2^16 even n over the range; sieve terms as in the SOL")},
             "hbm": {"achieved": hbm_bytes / k_s / 1e9, "peak": hbm, "unit": "GB/s",
                     "frac": hbm_bytes / k_s / 1e9 / hbm, "peak_source": hbm_kind,
                     "note": "q-bitset bytes a staged design would move; the fused kernel keeps them on chip"}},

@@ -90,9 +90,19 @@ static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, cons
     d.g0 = host_window_g0(d.start, H);
     d.orig = i;
     const uint64_t chunks = (d.count + NE - 1) / NE;
-    const int64_t g_last = host_window_g0(d.start + 2 * (uint64_t)NE * (chunks - 1), H);
-    // every chunk reads nbw + 1 mask words from its own base on
-    const uint64_t lw = ((uint64_t)(g_last - d.g0) >> 5) + nbw + 2;
+    // a chunk reads nwords + 1 mask words from its own base on (nwords as in
+    // range6_kernel: the words its search can read for a real n); the mask
+    // ends there, so the large-prime pass marks no bit nobody reads
+    auto reach = [&](uint64_t ci) {  // mask words chunk ci reads, from the window base
+      const uint64_t cnt = std::min<uint64_t>(NE, d.count - ci * NE);
+      const uint64_t nbits = H / 6 + cnt / 3 + 96;
+      const uint64_t nwords = std::min<uint64_t>(nbw, (nbits + 31) / 32 + 2);
+      const int64_t gc = host_window_g0(d.start + 2 * (uint64_t)NE * ci, H);
+      return ((uint64_t)(gc - d.g0) >> 5) + nwords + 2;
+    };
+    // the last full chunk or the (possibly short) last one reaches furthest
+    uint64_t lw = reach(chunks - 1);
+    if (chunks >= 2) lw = std::max(lw, reach(chunks - 2));
     d.lwords = (uint32_t)((lw + 3) & ~3ull);
     d.lbase = lwords_total;
     lwords_total += 2ull * d.lwords;

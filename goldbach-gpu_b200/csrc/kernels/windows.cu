@@ -71,41 +71,93 @@ __device__ __noinline__ void win_mark_from(const WinLargeArgs& a, uint32_t w, ui
   for (uint32_t i = t5; i < lbits; i += p) atomicAnd(&L5[i >> 5], ~(1u << (i & 31)));
 }
 
+// First window w in [w_lo, w_hi) whose top reaches p^2 (windows sorted by
+// q_top).
+__device__ __forceinline__ uint32_t first_window(const WinLargeArgs& a, uint64_t pp) {
+  uint32_t lo = a.w_lo, hi = a.w_hi;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (a.win[mid].q_top < pp) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Per-prime constants of the fast path.
+struct LargePrime {
+  uint32_t p, a1, dl;  // prime, -1/6 mod p, (a5 - a1) mod p
+  double inv;
+};
+
+__device__ __forceinline__ LargePrime large_prime(const WinLargeArgs& a, uint32_t k) {
+  LargePrime q;
+  q.p = __ldg(a.primes + k);
+  const uint2 ac = __ldg(a.a15 + k);
+  q.a1 = ac.x;
+  q.dl = ac.y >= ac.x ? ac.y - ac.x : ac.y + q.p - ac.x;
+  q.inv = 1.0 / (double)q.p;
+  return q;
+}
+
+// One (prime, window) pair on the fast path (p < 2^31): the first marks of
+// both classes from the quotient estimate, and the marking when one falls
+// inside the mask (or the exact path for a window flagged for it).
+__device__ __forceinline__ void large_pair(const WinLargeArgs& a, const WinLarge& v, uint32_t w,
+                                           const LargePrime& q, uint32_t k) {
+  const double kRound = 6755399441055744.0;  // 1.5 * 2^52
+  const uint32_t qe = (uint32_t)__double_as_longlong(fma(v.gd, q.inv, kRound));
+  uint32_t r = v.gl - qe * q.p;  // g0 - p round(g0 / p), in (-p, p)
+  r = min(r, r + q.p);           // [0, p)
+  uint32_t t1 = q.a1 - r;
+  t1 = min(t1, t1 + q.p);
+  uint32_t t5 = t1 + q.dl;
+  t5 = min(t5, t5 - q.p);
+  if (min(t1, t5) < v.lbits) {  // a mark in the window, or the exact path
+    if (v.lbits == 0xffffffffu) win_mark_exact(a, w, q.p, k);
+    else win_mark_from(a, w, q.p, t1, t5, v.lbits);
+  }
+}
+
+// One prime over its windows (any p < 2^32).
+__device__ __noinline__ void large_one(const WinLargeArgs& a, uint32_t k) {
+  const uint32_t p = __ldg(a.primes + k);
+  const uint32_t lo = first_window(a, (uint64_t)p * p);
+  if (p >= 0x80000000u) {  // windows near 2^64 only: every pair exact
+    for (uint32_t w = lo; w < a.w_hi; ++w) win_mark_exact(a, w, p, k);
+    return;
+  }
+  const LargePrime q = large_prime(a, k);
+  for (uint32_t w = lo; w < a.w_hi; ++w) large_pair(a, a.wl[w], w, q, k);
+}
+
+// Each thread takes kLargePPT consecutive primes (close in size, so their
+// first windows nearly agree) and walks the windows once for all of them:
+// one record load per kLargePPT pairs and kLargePPT independent chains.
+constexpr uint32_t kLargePPT = 4;
+
 __global__ void __launch_bounds__(kWinLargeThreads) win_large_kernel(const __grid_constant__ WinLargeArgs a) {
-  const uint32_t stride = gridDim.x * kWinLargeThreads;
-  for (uint32_t k = a.k0 + blockIdx.x * kWinLargeThreads + threadIdx.x; k < a.k1; k += stride) {
-    const uint32_t p = __ldg(a.primes + k);
-    const uint64_t pp = (uint64_t)p * p;
-    // first window whose top reaches p^2 (windows sorted by q_top)
-    uint32_t lo = a.w_lo, hi = a.w_hi;
-    while (lo < hi) {
-      const uint32_t mid = (lo + hi) >> 1;
-      if (a.win[mid].q_top < pp) lo = mid + 1;
-      else hi = mid;
-    }
-    if (p >= 0x80000000u) {  // windows near 2^64 only: every pair exact
-      for (uint32_t w = lo; w < a.w_hi; ++w) win_mark_exact(a, w, p, k);
+  const uint32_t stride = gridDim.x * kWinLargeThreads * kLargePPT;
+  for (uint32_t k = a.k0 + (blockIdx.x * kWinLargeThreads + threadIdx.x) * kLargePPT; k < a.k1;
+       k += stride) {
+    if (k + kLargePPT > a.k1 || __ldg(a.primes + k + kLargePPT - 1) >= 0x80000000u) {
+      for (uint32_t j = k; j < k + kLargePPT && j < a.k1; ++j) large_one(a, j);
       continue;
     }
-    const double inv = 1.0 / (double)p;
-    const uint2 ac = __ldg(a.a15 + k);
-    const uint32_t a1 = ac.x;
-    const uint32_t dl = ac.y >= ac.x ? ac.y - ac.x : ac.y + p - ac.x;  // a5 - a1 mod p
-    const double kRound = 6755399441055744.0;                         // 1.5 * 2^52
-#pragma unroll 4
-    for (uint32_t w = lo; w < a.w_hi; ++w) {
+    LargePrime q[kLargePPT];
+    uint32_t lo[kLargePPT];
+#pragma unroll
+    for (uint32_t j = 0; j < kLargePPT; ++j) {
+      q[j] = large_prime(a, k + j);
+      lo[j] = first_window(a, (uint64_t)q[j].p * q[j].p);
+    }
+    // lo[0] is the smallest (p ascending); a pair before a prime's own first
+    // window is skipped
+#pragma unroll 2
+    for (uint32_t w = lo[0]; w < a.w_hi; ++w) {
       const WinLarge v = a.wl[w];
-      const uint32_t qe = (uint32_t)__double_as_longlong(fma(v.gd, inv, kRound));
-      uint32_t r = v.gl - qe * p;  // g0 - p round(g0 / p), in (-p, p)
-      r = min(r, r + p);           // [0, p)
-      uint32_t t1 = a1 - r;
-      t1 = min(t1, t1 + p);
-      uint32_t t5 = t1 + dl;
-      t5 = min(t5, t5 - p);
-      if (min(t1, t5) < v.lbits) {  // a mark in the window, or the exact path
-        if (v.lbits == 0xffffffffu) win_mark_exact(a, w, p, k);
-        else win_mark_from(a, w, p, t1, t5, v.lbits);
-      }
+#pragma unroll
+      for (uint32_t j = 0; j < kLargePPT; ++j)
+        if (w >= lo[j]) large_pair(a, v, w, q[j], k + j);
     }
   }
 }
