@@ -243,7 +243,7 @@ def seeded_windows(seed=1, count=4096, lo=10**15, hi=10**18, wlo=10, whi=24):
     return starts, np.maximum(widths, 1)
 
 
-def measure_windows(gb, ctx, nwin=4096, plain=True):
+def measure_windows(gb, ctx, nwin=4096, plain=True, tune=True):
     """C3: the whole batch in one persistent pipeline, and the plain
     per-window pipeline on the same 4096 windows; the per-window results of
     the two must be identical.  (nwin < 4096 and plain=False: the first nwin
@@ -251,14 +251,19 @@ def measure_windows(gb, ctx, nwin=4096, plain=True):
     starts, counts = seeded_windows()
     starts, counts = starts[:nwin], counts[:nwin]
     ctx.verify_windows(starts[:64], counts[:64])  # warm-up (tables to 1e9)
+    knobs = {}
+    if tune:  # the batch class's knobs (timed on a sample)
+        tune = ctx.autotune_windows(starts, counts)
+        knobs = {k: tune[k] for k in ("mr_divisor", "large_ctas_per_sm", "block_threads")}
+        knobs["chunk"] = tune["chunk_evens"]
     if plain:
         ctx.verify_windows(starts[:64], counts[:64], mode=gb.GB_WINDOWS_PLAIN)
     t0 = time.perf_counter()
-    per, _, s = ctx.verify_windows(starts, counts, mode=gb.GB_WINDOWS_PERSISTENT)
+    per, _, s = ctx.verify_windows(starts, counts, mode=gb.GB_WINDOWS_PERSISTENT, **knobs)
     wall = time.perf_counter() - t0
     total = int(counts.sum())
     t1 = time.perf_counter()
-    per_p, _, sp = (ctx.verify_windows(starts, counts, mode=gb.GB_WINDOWS_PLAIN) if plain
+    per_p, _, sp = (ctx.verify_windows(starts, counts, mode=gb.GB_WINDOWS_PLAIN, **knobs) if plain
                     else (per, None, s))
     wall_p = time.perf_counter() - t1
     same = per == per_p
@@ -274,7 +279,7 @@ def measure_windows(gb, ctx, nwin=4096, plain=True):
             "plain_windows": len(starts), "plain_ms": sp["device_ms"], "plain_value": pv,
             "plain_launches": sp["kernel_launches"], "batched_over_plain": v / pv,
             "identical_results": bool(same), "failures": s["failures"],
-            "sieved_windows": s["sieved_windows"], "large_pairs": s["large_pairs"],
+            "autotuned": tune, "sieved_windows": s["sieved_windows"], "large_pairs": s["large_pairs"],
             "large_ms": s["large_ms"], "search_ms": s["search_ms"],
             "roofline": {"bound": "int", "kernel": "win_large_kernel",
                          "achieved": ops / large_s / 1e12 if large_s else None,
@@ -418,6 +423,48 @@ def measure_counts(gb, ctx, points=((10**9, 4096), (10**10, 1024))):
     return out
 
 
+# the reference's published flags for its GPU verifier (RESULTS.md:39-41)
+REF_GPU_FLAGS = ["--seg-size=200000000", "--p-small=1000000", "--batch-size=2000000"]
+
+
+def measure_reference_gpu(gb, ctx, device, limits=(10**9, 10**10, 10**11)):
+    """The reference's own GPU verifier (src/goldbach.cu built unmodified for
+    sm_100a into oracle/_ref/goldbach) on this B200 with its published flags:
+    its printed "Total computation time" (the worker threads' span), beside
+    the wall time and device time of this build's gb_verify_range over the
+    same [4, LIMIT].  Timing only: the reference's tiled sieve updates shared
+    memory without synchronisation, so its answers are not a check."""
+    import re
+    exe = os.path.join(ROOT, "oracle", "_ref", "goldbach")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/goldbach not built (oracle/build_ref.sh)"}
+    out = []
+    for lim in limits:
+        clk = ClockSampler(device)
+        clk.start()
+        try:
+            r = subprocess.run([exe, str(lim)] + REF_GPU_FLAGS, capture_output=True, text=True,
+                               timeout=600)
+            txt, rc = r.stdout, r.returncode
+        except subprocess.TimeoutExpired:
+            txt, rc = "", "timeout"
+        clocks = clk.stop()
+        m = re.search(r"Total computation time : ([0-9.eE+-]+) seconds", txt)
+        fb = re.search(r"Phase 2 fallbacks\s+: (\d+)", txt)
+        ctx.verify_range(4, lim)  # warm (tables)
+        t0 = time.perf_counter()
+        ours = ctx.verify_range(4, lim).result
+        wall = time.perf_counter() - t0
+        ref_s = float(m.group(1)) if m else None
+        out.append({"limit": lim, "flags": " ".join(REF_GPU_FLAGS), "rc": rc,
+                    "reference_s": ref_s, "reference_fallbacks": int(fb.group(1)) if fb else None,
+                    "reference_says_verified": "satisfy Goldbach" in txt, "reference_clocks": clocks,
+                    "ours_wall_s": wall, "ours_device_s": ours["device_ms"] / 1e3,
+                    "ours_failures": ours["failures"],
+                    "speedup_wall": (ref_s / wall) if ref_s else None})
+    return out
+
+
 # serving lanes poll their queues this long before blocking (one host core
 # per lane kept busy; single-request p50 at 1e3 requests/s 58 against 74 us)
 SERVE_SPIN_US = 20000
@@ -492,15 +539,20 @@ def main():
     ap.add_argument("--seg-size", type=int, default=1 << 27)
     ap.add_argument("--chunk", type=int, default=0)
     ap.add_argument("--halo", type=int, default=0)
+    ap.add_argument("--block-threads", type=int, default=0)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default chunk / halo / block shape instead of the autotuner's")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--ref-sample-log2", type=int, default=24)
-    ap.add_argument("--extra", choices=["windows", "single", "counts", "serving"],
+    ap.add_argument("--extra", choices=["windows", "single", "counts", "serving", "reference_gpu"],
                     help="run only this secondary measurement and print its JSON (profiling)")
     ap.add_argument("--windows", type=int, default=4096,
                     help="--extra windows: the first N seeded windows only")
     ap.add_argument("--no-windows-plain", action="store_true",
                     help="--extra windows: skip the plain per-window pipeline")
+    ap.add_argument("--no-windows-tune", action="store_true",
+                    help="--extra windows: default knobs instead of the windows autotuner's")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -511,7 +563,10 @@ def main():
         else:
             with gb.Context(0) as c:
                 if args.extra == "windows":
-                    print(json.dumps(measure_windows(gb, c, args.windows, not args.no_windows_plain)))
+                    print(json.dumps(measure_windows(gb, c, args.windows, not args.no_windows_plain,
+                                                     not args.no_windows_tune)))
+                elif args.extra == "reference_gpu":
+                    print(json.dumps(measure_reference_gpu(gb, c, 0)))
                 else:
                     f = {"single": measure_single, "counts": measure_counts}
                     print(json.dumps(f[args.extra](gb, c)))
@@ -542,7 +597,15 @@ def main():
     segfb = torch.zeros(nseg, dtype=torch.int32, device=dev)
     segfail = torch.zeros(nseg, dtype=torch.int32, device=dev)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+    # chunk, halo and block shape: the autotuner's choice for this range class
+    # (timed once on the top 2^28 n, outside the timed region), unless given
+    tune = {}
+    if not (args.chunk or args.halo or args.no_autotune):
+        tune = ctx.autotune_range(start, limit, seg_size=args.seg_size)
+        args.chunk, args.halo = tune["chunk_evens"], tune["halo"]
+        args.block_threads = tune["block_threads"]
     kw = dict(seg_size=args.seg_size, chunk=args.chunk, halo=args.halo, shard_index=rank,
+              block_threads=args.block_threads,
               shard_count=world, stream=stream.cuda_stream)
 
     def barrier():
@@ -592,7 +655,7 @@ def main():
 
     def step_host():
         o = gb.RangeOpts(args.seg_size, 10**6, 0, args.chunk, args.halo, rank, world, 0,
-                         stream.cuda_stream)
+                         stream.cuda_stream, args.block_threads)
         out = gb.RangeOut(None, None, h_hist.data_ptr(), h_fb.data_ptr(), h_fail.data_ptr(), None)
         res = gb.RangeResult()
         st = L.gb_verify_range(ctx._h, start, limit, ctypes.byref(o), ctypes.byref(res), ctypes.byref(out))
@@ -649,7 +712,8 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": f"range [{start}, {limit}] (every even n)", "seg_size": args.seg_size,
-                   "chunk_evens": chunk, "halo": halo, "p_small": 10**6, "phase2_limit": 10**8,
+                   "chunk_evens": chunk, "halo": halo, "block_threads": args.block_threads or 512,
+                   "autotuned": tune or None, "p_small": 10**6, "phase2_limit": 10**8,
                    "l2": "flushed (512 MB write) between steps",
                    "parallelism": f"segments sharded over {world} GPU(s)"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h},
@@ -686,6 +750,7 @@ def main():
             out["cpu_baseline"] = cpu_baseline_oracle(limit)
         if not args.no_extras:
             with gb.Context(local) as c2:
+                out["reference_gpu"] = measure_reference_gpu(gb, c2, local)
                 out["windows"] = measure_windows(gb, c2)
                 out["single"] = measure_single(gb, c2)
                 out["counts"] = measure_counts(gb, c2)

@@ -43,12 +43,14 @@ class Config(C.Structure):
 class RangeOpts(C.Structure):
     _fields_ = [("seg_size", u64), ("p_small", u64), ("phase2_limit", u64),
                 ("chunk_evens", u32), ("halo", u32), ("shard_index", u32),
-                ("shard_count", u32), ("on_device", i32), ("stream", vp)]
+                ("shard_count", u32), ("on_device", i32), ("stream", vp),
+                ("block_threads", u32)]
 
 
 class AutotuneResult(C.Structure):
-    _fields_ = [("chunk_evens", u32), ("halo", u32), ("even_n_per_s", C.c_double),
-                ("candidates", u32), ("sample_evens", u64), ("cached", i32)]
+    _fields_ = [("chunk_evens", u32), ("halo", u32), ("block_threads", u32),
+                ("even_n_per_s", C.c_double), ("candidates", u32), ("sample_evens", u64),
+                ("cached", i32)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -88,7 +90,17 @@ class Window(C.Structure):
 
 class WindowsOpts(C.Structure):
     _fields_ = [("mode", i32), ("chunk_evens", u32), ("halo", u32),
-                ("phase2_limit", u64), ("on_device", i32), ("stream", vp), ("mr_below", u64)]
+                ("phase2_limit", u64), ("on_device", i32), ("stream", vp), ("mr_below", u64),
+                ("mr_divisor", u32), ("large_ctas_per_sm", u32), ("block_threads", u32)]
+
+
+class WindowsTune(C.Structure):
+    _fields_ = [("mr_divisor", u32), ("chunk_evens", u32), ("large_ctas_per_sm", u32),
+                ("block_threads", u32), ("even_n_per_s", C.c_double), ("candidates", u32),
+                ("sample_windows", u32), ("cached", i32)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
 
 
 class WindowResult(C.Structure):
@@ -158,6 +170,8 @@ def load(path: str = LIB_PATH):
         "gb_sieve_bitset": (i32, [vp, u64, u64, vp, i32, vp]),
         "gb_goldbach_counts": (i32, [vp, u64, u64, vp, P(CountOpts)]),
         "gb_autotune_range": (i32, [vp, u64, u64, P(RangeOpts), P(RangeOpts), P(AutotuneResult)]),
+        "gb_autotune_windows": (i32, [vp, P(Window), C.c_size_t, P(WindowsOpts), P(WindowsOpts),
+                                      P(WindowsTune)]),
         "gb_primes_upto": (i32, [vp, u64, vp, u64, P(u64)]),
         "gb_is_prime_batch": (i32, [vp, vp, C.c_size_t, vp, i32, vp]),
         "gb_check_single_batch": (i32, [vp, vp, C.c_size_t, vp, vp, P(SingleOpts), P(SingleResult)]),
@@ -245,7 +259,7 @@ class Context:
                        p_small: int = 1_000_000, phase2_limit: int = 0) -> dict:
         """gb_autotune_range: the chunk_evens and halo to use for [start, limit]
         (timed on a sample at the top of the range, cached per range class)."""
-        base = RangeOpts(seg_size, p_small, phase2_limit, 0, 0, 0, 1, 0, None)
+        base = RangeOpts(seg_size, p_small, phase2_limit, 0, 0, 0, 1, 0, None, 0)
         tuned = RangeOpts()
         r = AutotuneResult()
         self._check(self.L.gb_autotune_range(self._h, start, limit, C.byref(base), C.byref(tuned),
@@ -257,7 +271,7 @@ class Context:
                      halo: int = 0, shard_index: int = 0, shard_count: int = 1,
                      want_minp=False, want_bits=False, want_hist=True, want_seg=False,
                      want_seg_hist=False, stream=None, device_out: dict | None = None,
-                     check: bool = True) -> RangeRun:
+                     check: bool = True, block_threads: int = 0) -> RangeRun:
         """Verifies every even n in [start, limit].  Host numpy outputs are
         allocated on request; `device_out` maps RangeOut field names to device
         pointers (torch tensors) and switches the call to on_device mode."""
@@ -267,7 +281,7 @@ class Context:
         count = (lim - st0) // 2 + 1 if lim >= st0 else 0
         nseg = L.gb_num_segments(start, limit, seg_size)
         o = RangeOpts(seg_size, p_small, phase2_limit, chunk, halo, shard_index, shard_count,
-                      0, stream or None)
+                      0, stream or None, block_threads)
         run = RangeRun(result={})
         out = RangeOut()
         if device_out is not None:
@@ -351,19 +365,39 @@ class Context:
         return p, q, r
 
     # -- windows -------------------------------------------------------------
-    def verify_windows(self, starts, counts, *, mode=GB_WINDOWS_PERSISTENT, chunk=0, halo=0,
-                       phase2_limit=0, want_minp=False, stream=None, mr_below=0):
+    @staticmethod
+    def _windows(starts, counts):
         starts = np.asarray(starts, dtype=np.uint64)
         counts = np.asarray(counts, dtype=np.uint64)
-        nw = len(starts)
-        w = (Window * nw)()
-        for i in range(nw):
+        w = (Window * len(starts))()
+        for i in range(len(starts)):
             w[i].start = int(starts[i])
             w[i].count = int(counts[i])
+        return w
+
+    def autotune_windows(self, starts, counts, phase2_limit=0) -> dict:
+        """gb_autotune_windows: the Miller-Rabin split divisor, chunk, large-prime
+        grid and block shape for this batch (timed on a sample, cached per
+        batch class); the dict carries the choice and the opts to pass on."""
+        w = self._windows(starts, counts)
+        base = WindowsOpts(GB_WINDOWS_PERSISTENT, 0, 0, phase2_limit, 0, None, 0, 0, 0, 0)
+        tuned = WindowsOpts()
+        r = WindowsTune()
+        self._check(self.L.gb_autotune_windows(self._h, w, len(w), C.byref(base), C.byref(tuned),
+                                               C.byref(r)))
+        return r.as_dict()
+
+    def verify_windows(self, starts, counts, *, mode=GB_WINDOWS_PERSISTENT, chunk=0, halo=0,
+                       phase2_limit=0, want_minp=False, stream=None, mr_below=0, mr_divisor=0,
+                       large_ctas_per_sm=0, block_threads=0):
+        counts = np.asarray(counts, dtype=np.uint64)
+        w = self._windows(starts, counts)
+        nw = len(w)
         res = (WindowResult * nw)()
         minp = np.zeros(int(counts.sum()), np.uint32) if want_minp else None
         s = WindowsSummary()
-        o = WindowsOpts(mode, chunk, halo, phase2_limit, 0, stream or None, mr_below)
+        o = WindowsOpts(mode, chunk, halo, phase2_limit, 0, stream or None, mr_below, mr_divisor,
+                        large_ctas_per_sm, block_threads)
         self._check(self.L.gb_verify_windows(self._h, w, nw, C.byref(o), res,
                                              _ptr(minp), C.byref(s)))
         per = [{f: getattr(res[i], f) for f, _ in WindowResult._fields_} for i in range(nw)]

@@ -119,7 +119,7 @@ int main(int argc, char** argv) {
   }
   bool show_progress = false, json = false, counts_mode = false;
   uint64_t LIMIT = 0, SEG_SIZE = 10'000'000ULL, P_SMALL = 1'000'000ULL, START = 4;
-  uint64_t chunk = 0, halo = 0, phase2 = 0, mem_mb = 0, batch = 100000;
+  uint64_t chunk = 0, halo = 0, phase2 = 0, mem_mb = 0, batch = 100000, threads = 0;
   std::string journal_path, tune_cache, minp_path, bitmap_path;
   bool autotune = false;
   uint64_t journal_segs = 0, stop_after = 0;
@@ -329,7 +329,8 @@ int main(int argc, char** argv) {
   }
   std::cout << "Pre-generating device primes up to " << std::max(P_SMALL, p2) << "...\n";
   if (autotune) {
-    // one line per range class: "class BITS P_SMALL PHASE2 chunk C halo H"
+    // one line per range class: "class BITS P_SMALL PHASE2 chunk C halo H
+    // threads T" (a line without the threads field keeps the default shape)
     uint64_t bits = 0;
     for (uint64_t x = LIMIT; x; x >>= 1) ++bits;
     char key[128];
@@ -339,16 +340,19 @@ int main(int argc, char** argv) {
       std::ifstream in(tune_cache);
       std::string line;
       while (std::getline(in, line)) {
-        unsigned long long c = 0, h = 0;
+        unsigned long long c = 0, h = 0, t = 0;
         const size_t at = line.find(" chunk ");
         if (at != std::string::npos && line.substr(0, at) == key &&
-            std::sscanf(line.c_str() + at, " chunk %llu halo %llu", &c, &h) == 2) {
+            std::sscanf(line.c_str() + at, " chunk %llu halo %llu threads %llu", &c, &h, &t) >= 2) {
           chunk = c;
           halo = h;
+          threads = t;
           found = true;
         }
       }
-      if (found) std::cout << "[Autotune] chunk=" << chunk << " halo=" << halo << " (from " << tune_cache << ")\n";
+      if (found)
+        std::cout << "[Autotune] chunk=" << chunk << " halo=" << halo << " threads=" << threads
+                  << " (from " << tune_cache << ")\n";
     }
     if (!found) {
       gb_range_opts base{}, tuned{};
@@ -363,15 +367,17 @@ int main(int argc, char** argv) {
       }
       chunk = tuned.chunk_evens;
       halo = tuned.halo;
+      threads = tuned.block_threads;
       if (ar.candidates)
-        std::cout << "[Autotune] chunk=" << chunk << " halo=" << halo << " (" << std::scientific
+        std::cout << "[Autotune] chunk=" << chunk << " halo=" << halo << " threads=" << threads
+                  << " (" << std::scientific
                   << std::setprecision(3) << ar.even_n_per_s << " n/s on " << ar.sample_evens
                   << " n, " << ar.candidates << " candidates)\n" << std::defaultfloat << std::setprecision(6);
       else
         std::cout << "[Autotune] range too short to tune: defaults\n";
       if (!tune_cache.empty() && ar.candidates) {
         std::ofstream out(tune_cache, std::ios::app);
-        out << key << " chunk " << chunk << " halo " << halo << "\n";
+        out << key << " chunk " << chunk << " halo " << halo << " threads " << threads << "\n";
       }
     }
   }
@@ -419,6 +425,7 @@ int main(int argc, char** argv) {
       o.phase2_limit = p2;
       o.chunk_evens = (uint32_t)chunk;
       o.halo = (uint32_t)halo;
+      o.block_threads = (uint32_t)threads;
       uint64_t a = START, e = LIMIT;
       if (single_call) {
         o.shard_index = g;

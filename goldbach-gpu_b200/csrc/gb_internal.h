@@ -87,6 +87,7 @@ struct RangeArgs {
   uint64_t chunks_per_seg; // ceil(seg_size / chunk_evens)
   uint64_t total_items;    // (segments of this shard) * chunks_per_seg
   uint32_t chunk_evens;    // NE
+  uint32_t threads;        // block size of range6_kernel: 256, 512 or 1024 (0: 512)
   uint32_t nbw;            // words of the q-window bitset (incl. padding)
   const uint64_t* magic;   // Barrett reciprocals, magic[k] for primes[k]
   uint32_t nsieve;         // primes[kWheelPrimeCount+1 .. nsieve) mark the window

@@ -325,6 +325,8 @@ gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint
   }
   if (NE < 8192 || NE > (1u << 20) || (NE & (NE - 1)))
     return fail(w, GB_EINVAL, "chunk_evens must be a power of two in [2^13, 2^20]");
+  if (o.block_threads && o.block_threads != 256 && o.block_threads != 512 && o.block_threads != 1024)
+    return fail(w, GB_EINVAL, "block_threads must be 256, 512 or 1024");
   const uint32_t sc = o.shard_count ? o.shard_count : 1;
   if (o.shard_index >= sc) return fail(w, GB_EINVAL, "shard_index >= shard_count");
   const uint64_t nseg = (count + o.seg_size - 1) / o.seg_size;
@@ -345,6 +347,7 @@ gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint
   a.chunks_per_seg = cps;
   a.total_items = my_segs * cps;
   a.chunk_evens = NE;
+  a.threads = o.block_threads;
   // two class bitsets of H/6 + NE/3 bits (plus the over-read of the last
   // warp task); primes p <= H - 13 keep every q = n - p in the window
   a.nbw = range6_words(H, NE);
@@ -781,8 +784,10 @@ static gb_status autotune_impl(gb_ctx* c, Workspace& w, uint64_t start, uint64_t
   if (it != c->tuned.end()) {
     tuned->chunk_evens = it->second.chunk;
     tuned->halo = it->second.halo;
+    tuned->block_threads = it->second.threads;
     r.chunk_evens = it->second.chunk;
     r.halo = it->second.halo;
+    r.block_threads = it->second.threads;
     r.even_n_per_s = it->second.rate;
     r.cached = 1;
     if (res) *res = r;
@@ -798,24 +803,28 @@ static gb_status autotune_impl(gb_ctx* c, Workspace& w, uint64_t start, uint64_t
   gb_status st = range_impl(c, w, nullptr, s0, limit, &t, &rr, nullptr);  // warm-up
   if (st != GB_OK) return st;
   double best = -1;
-  for (uint32_t chunk : {1u << 18, 1u << 19, 1u << 20})
-    for (uint32_t halo : {1u << 14, 1u << 15, 1u << 16}) {
-      t.chunk_evens = chunk;
-      t.halo = halo;
-      if ((st = range_impl(c, w, nullptr, s0, limit, &t, &rr, nullptr)) != GB_OK) return st;
-      ++r.candidates;
-      const double rate = rr.kernel_ms > 0 ? sample / (rr.kernel_ms / 1e3) : 0;
-      if (rate > best) {
-        best = rate;
-        r.chunk_evens = chunk;
-        r.halo = halo;
+  for (uint32_t threads : {512u, 256u, 1024u})
+    for (uint32_t chunk : {1u << 18, 1u << 19, 1u << 20})
+      for (uint32_t halo : {1u << 14, 1u << 15, 1u << 16}) {
+        t.chunk_evens = chunk;
+        t.halo = halo;
+        t.block_threads = threads;
+        if ((st = range_impl(c, w, nullptr, s0, limit, &t, &rr, nullptr)) != GB_OK) return st;
+        ++r.candidates;
+        const double rate = rr.kernel_ms > 0 ? sample / (rr.kernel_ms / 1e3) : 0;
+        if (rate > best) {
+          best = rate;
+          r.chunk_evens = chunk;
+          r.halo = halo;
+          r.block_threads = threads;
+        }
       }
-    }
   r.even_n_per_s = best;
   r.sample_evens = sample;
-  c->tuned[key] = gb_ctx::Tuned{r.chunk_evens, r.halo, best};
+  c->tuned[key] = gb_ctx::Tuned{r.chunk_evens, r.halo, r.block_threads, best};
   tuned->chunk_evens = r.chunk_evens;
   tuned->halo = r.halo;
+  tuned->block_threads = r.block_threads;
   if (res) *res = r;
   return GB_OK;
 }
@@ -824,6 +833,12 @@ gb_status gb_autotune_range(gb_ctx* c, uint64_t start, uint64_t limit, const gb_
                             gb_range_opts* tuned, gb_autotune_result* res) {
   if (!c) return GB_EINVAL;
   GB_PUBLIC(c, autotune_impl(c, c->ws, start, limit, base, tuned, res));
+}
+
+gb_status gb_autotune_windows(gb_ctx* c, const gb_window* w, size_t count, const gb_windows_opts* base,
+                              gb_windows_opts* tuned, gb_windows_tune* res) {
+  if (!c) return GB_EINVAL;
+  GB_PUBLIC(c, autotune_windows_impl(c, c->ws, w, count, base, tuned, res));
 }
 
 // Partition counts (kernels/counts.cu): the odd-prime bitset of [1, n_max]

@@ -84,12 +84,15 @@ struct gb_ctx {
   gb::Workspace ws;  // the public entry points' workspace
   gb_server* server = nullptr;
   // gb_autotune_range's choices per range class (bit length of the limit,
-  // p_small, phase2_limit) -> (chunk_evens, halo, even n/s)
+  // p_small, phase2_limit) -> (chunk_evens, halo, block threads, even n/s)
   struct Tuned {
-    uint32_t chunk, halo;
+    uint32_t chunk, halo, threads;
     double rate;
   };
   std::map<std::vector<uint64_t>, Tuned> tuned;
+  // gb_autotune_windows's choices per batch class (bit length of the
+  // largest top, bit length of the window count)
+  std::map<std::vector<uint64_t>, gb_windows_tune> tuned_windows;
 };
 
 namespace gb {
@@ -137,6 +140,9 @@ gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint
 gb_status single_impl(gb_ctx* c, Workspace& w, Arena* arena, const uint64_t* n, size_t count,
                       uint64_t* p_out, uint64_t* q_out, const gb_single_opts* opts,
                       gb_single_result* res);
+gb_status autotune_windows_impl(gb_ctx* c, Workspace& w, const gb_window* win, size_t count,
+                                const gb_windows_opts* base, gb_windows_opts* tuned,
+                                gb_windows_tune* res);
 gb_status windows_impl(gb_ctx* c, Workspace& w, Arena* arena, const gb_window* win, size_t count,
                        const gb_windows_opts* opts, gb_window_result* res, uint32_t* min_p_concat,
                        gb_windows_summary* sum);

@@ -52,8 +52,11 @@ static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, cons
   const uint32_t NE = o.chunk_evens ? o.chunk_evens : (1u << 20);
   if (NE < 8192 || NE > (1u << 20) || (NE & (NE - 1)))
     return fail(ws, GB_EINVAL, "chunk_evens must be a power of two in [2^13, 2^20]");
+  if (o.block_threads && o.block_threads != 256 && o.block_threads != 512 && o.block_threads != 1024)
+    return fail(ws, GB_EINVAL, "block_threads must be 256, 512 or 1024");
   const uint64_t p_lim = o.phase2_limit ? o.phase2_limit : GB_PHASE2_LIMIT_DEFAULT;
   if (p_lim > GB_P_SMALL_MAX) return fail(ws, GB_EINVAL, "phase2_limit must be <= 4e9");
+  const uint64_t large_per_sm = o.large_ctas_per_sm ? o.large_ctas_per_sm : kLargeBlocksPerSM;
   uint64_t total_n = 0, q_max = 0;
   for (size_t i = 0; i < count; ++i) {
     if (w[i].start < 4 || (w[i].start & 1) || w[i].count == 0)
@@ -150,6 +153,7 @@ static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, cons
   sp.queue = ws.queue;
   sp.queue_cap = ws.queue_cap;
   a.chunk_evens = NE;
+  a.threads = o.block_threads;
   a.nbw = nbw;
   a.magic = c->d_magic;
   a.nsieve = (uint32_t)std::max<uint64_t>(nsmall, kWheelPrimeCount + 1);
@@ -184,7 +188,7 @@ static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, cons
     a.surv = (uint2*)p;
   }
   const uint64_t np = la.k1 - la.k0;
-  const int gl = (int)std::max<uint64_t>(1, std::min<uint64_t>((np + 255) / 256, (uint64_t)sm * kLargeBlocksPerSM));
+  const int gl = (int)std::max<uint64_t>(1, std::min<uint64_t>((np + 255) / 256, (uint64_t)sm * large_per_sm));
 
   cudaStream_t s = o.stream ? (cudaStream_t)o.stream : c->stream;
   cudaError_t e = cudaSuccess;
@@ -390,7 +394,8 @@ gb_status windows_impl(gb_ctx* c, Workspace& ws, Arena* arena, const gb_window* 
     uint64_t lim = o.mr_below;
     if (!lim) {
       const double r = std::sqrt((double)last);
-      lim = r > 1e4 ? (uint64_t)(1.1 * r / std::log(r) / kMrBelowDivisor) : 0;
+      const double div = o.mr_divisor ? (double)o.mr_divisor : kMrBelowDivisor;
+      lim = r > 1e4 ? (uint64_t)(1.1 * r / std::log(r) / div) : 0;
     }
     narrow[i] = w[i].count < lim;
     nn += narrow[i];
@@ -442,6 +447,79 @@ gb_status windows_impl(gb_ctx* c, Workspace& ws, Arena* arena, const gb_window* 
     sum->large_ms = sb.large_ms;
     sum->search_ms = sb.search_ms;
   }
+  return GB_OK;
+}
+
+// Autotuner of the windows pipeline: the persistent mode on a sample of the
+// batch (every k-th window, at most 512) for each candidate, after one
+// warm-up call; the fastest device time wins.  Cached per batch class.
+gb_status autotune_windows_impl(gb_ctx* c, Workspace& ws, const gb_window* w, size_t count,
+                                const gb_windows_opts* base, gb_windows_opts* tuned,
+                                gb_windows_tune* res) {
+  if (!tuned || (count && !w)) return fail(ws, GB_EINVAL, "null argument");
+  gb_windows_opts o{};
+  if (base) o = *base;
+  *tuned = o;
+  gb_windows_tune r{};
+  if (count == 0) {
+    if (res) *res = r;
+    return GB_OK;
+  }
+  uint64_t top = 0;
+  for (size_t i = 0; i < count; ++i) top = std::max<uint64_t>(top, w[i].start + 2 * (w[i].count - 1));
+  uint64_t tb = 0, cb = 0;
+  for (uint64_t x = top; x; x >>= 1) ++tb;
+  for (uint64_t x = count; x; x >>= 1) ++cb;
+  const std::vector<uint64_t> key{tb, cb, o.phase2_limit};
+  auto it = c->tuned_windows.find(key);
+  if (it != c->tuned_windows.end()) {
+    r = it->second;
+    r.candidates = 0;
+    r.cached = 1;
+  } else {
+    const size_t step = (count + 511) / 512;
+    std::vector<gb_window> smp;
+    for (size_t i = 0; i < count; i += step) smp.push_back(w[i]);
+    std::vector<gb_window_result> wr(smp.size());
+    gb_windows_opts t = o;
+    t.mode = GB_WINDOWS_PERSISTENT;
+    t.on_device = 0;
+    gb_windows_summary sum{};
+    gb_status st = windows_impl(c, ws, nullptr, smp.data(), smp.size(), &t, wr.data(), nullptr, &sum);
+    if (st != GB_OK) return st;  // warm-up (tables)
+    uint64_t n = 0;
+    for (const gb_window& x : smp) n += x.count;
+    double best = -1;
+    for (uint32_t div : {2600u, 1300u, 5200u})
+      for (uint32_t chunk : {1u << 20, 1u << 19})
+        for (uint32_t large : {64u, 16u})
+          for (uint32_t threads : {512u, 256u}) {
+            t.mr_divisor = div;
+            t.chunk_evens = chunk;
+            t.large_ctas_per_sm = large;
+            t.block_threads = threads;
+            if ((st = windows_impl(c, ws, nullptr, smp.data(), smp.size(), &t, wr.data(), nullptr,
+                                   &sum)) != GB_OK)
+              return st;
+            ++r.candidates;
+            const double rate = sum.device_ms > 0 ? n / (sum.device_ms / 1e3) : 0;
+            if (rate > best) {
+              best = rate;
+              r.mr_divisor = div;
+              r.chunk_evens = chunk;
+              r.large_ctas_per_sm = large;
+              r.block_threads = threads;
+            }
+          }
+    r.even_n_per_s = best;
+    r.sample_windows = (uint32_t)smp.size();
+    c->tuned_windows[key] = r;
+  }
+  tuned->mr_divisor = r.mr_divisor;
+  tuned->chunk_evens = r.chunk_evens;
+  tuned->large_ctas_per_sm = r.large_ctas_per_sm;
+  tuned->block_threads = r.block_threads;
+  if (res) *res = r;
   return GB_OK;
 }
 

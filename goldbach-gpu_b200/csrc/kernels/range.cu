@@ -29,9 +29,12 @@ namespace gb {
 // The fused kernel: the q-window is the two class bitsets Q1 / Q5 (no
 // multiple of 3 stored), and the n of a chunk are searched by class n mod 6.
 
-// threads per CTA and CTAs per SM of range6_kernel
-constexpr int kRange6Threads = 512;
-constexpr int kRange6Blocks = 2;
+// Block shapes of range6_kernel: NT threads per CTA, launch-bounded to
+// 1024 / NT CTAs per SM so that every shape gets 64 registers a thread.  The
+// default is 512 x 2 (two 2^20-n chunks of 101 KB in an SM's shared memory);
+// 256 x 4 fits chunks of 2^19 n or fewer, 1024 x 1 one chunk per SM.  The
+// autotuner picks among them per range class.
+constexpr int kRange6DefaultThreads = 512;
 
 // floor((A - H - 1) / 6) for A possibly below H
 __device__ __forceinline__ int64_t window_g0(uint64_t A, uint32_t H) {
@@ -50,8 +53,8 @@ __device__ __forceinline__ uint32_t find_item_window(const uint64_t* off, uint32
   return lo;
 }
 
-template <bool MINP>
-__global__ void __launch_bounds__(kRange6Threads, kRange6Blocks) range6_kernel(const __grid_constant__ RangeArgs a) {
+template <bool MINP, int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT) range6_kernel(const __grid_constant__ RangeArgs a) {
   const SearchParams& s = a.s;
   __shared__ unsigned long long s_item;
   // windows mode: the item's window and chunk, decoded by thread 0
@@ -61,7 +64,7 @@ __global__ void __launch_bounds__(kRange6Threads, kRange6Blocks) range6_kernel(c
   const int tid = threadIdx.x;
   Ctx6& cx = g_cx6;
   uint32_t* pat6 = smem6_pat();
-  for (uint32_t i = tid; i < kWheel6Words; i += kRange6Threads) pat6[i] = a.wheel6[i];
+  for (uint32_t i = tid; i < kWheel6Words; i += NT) pat6[i] = a.wheel6[i];
   if (tid == 0) {
     cx.nbw = a.nbw;
     cx.surv = a.surv + (size_t)blockIdx.x * 6 * a.surv_cap;
@@ -97,7 +100,7 @@ __global__ void __launch_bounds__(kRange6Threads, kRange6Blocks) range6_kernel(c
       }
       cx.maxk = 0;
     }
-    for (uint32_t i = tid; i < kSmemHistBins; i += kRange6Threads) HIST[i] = 0;
+    for (uint32_t i = tid; i < kSmemHistBins; i += NT) HIST[i] = 0;
     __syncthreads();
     const unsigned long long item = s_item;
     if (item >= a.total_items) break;
@@ -158,9 +161,9 @@ __global__ void __launch_bounds__(kRange6Threads, kRange6Blocks) range6_kernel(c
       lsh = (uint32_t)(d & 31);
     }
     // q <= n - 3: the chunk's last n bounds the sieve (A + 2 cnt could pass 2^64)
-    sieve_window6<kRange6Threads>(Q1, Q5, nwords, nbits, G0, A + 2ull * (cnt - 1), pat6, s.primes,
+    sieve_window6<NT>(Q1, Q5, nwords, nbits, G0, A + 2ull * (cnt - 1), pat6, s.primes,
                                  a.magic, a.a15, a.nsieve, a.kcoop, L1, L5, lsh);
-    search_chunk6<MINP, kRange6Threads>(s);
+    search_chunk6<MINP, NT>(s);
   }
 }
 
@@ -247,10 +250,28 @@ static int occupancy(K kernel, size_t smem, int threads) {
   return nb;
 }
 
+// The instantiation for a's block shape (threads 256, 512 or 1024) and
+// outputs, handed to f(kernel, threads).
+template <typename F>
+static cudaError_t with_range_kernel(const RangeArgs& a, F f) {
+  const uint32_t nt = a.threads ? a.threads : kRange6DefaultThreads;
+  const bool mp = a.s.minp != nullptr;
+  switch (nt) {
+    case 256: return mp ? f(range6_kernel<true, 256>, 256) : f(range6_kernel<false, 256>, 256);
+    case 512: return mp ? f(range6_kernel<true, 512>, 512) : f(range6_kernel<false, 512>, 512);
+    case 1024: return mp ? f(range6_kernel<true, 1024>, 1024) : f(range6_kernel<false, 1024>, 1024);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 int range_max_blocks_per_sm(const RangeArgs& a) {
   const size_t smem = range_smem_bytes(a);
-  return a.s.minp ? occupancy(range6_kernel<true>, smem, kRange6Threads)
-                  : occupancy(range6_kernel<false>, smem, kRange6Threads);
+  int nb = 0;
+  with_range_kernel(a, [&](auto kernel, int threads) {
+    nb = occupancy(kernel, smem, threads);
+    return cudaSuccess;
+  });
+  return nb;
 }
 
 template <typename K>
@@ -264,8 +285,9 @@ static cudaError_t launch_one(K kernel, const RangeArgs& a, int grid, size_t sme
 
 cudaError_t launch_range(const RangeArgs& a, int grid, cudaStream_t st) {
   const size_t smem = range_smem_bytes(a);
-  return a.s.minp ? launch_one(range6_kernel<true>, a, grid, smem, st, kRange6Threads)
-                  : launch_one(range6_kernel<false>, a, grid, smem, st, kRange6Threads);
+  return with_range_kernel(a, [&](auto kernel, int threads) {
+    return launch_one(kernel, a, grid, smem, st, threads);
+  });
 }
 
 cudaError_t launch_fallback(const SearchParams& s, int grid, cudaStream_t st) {

@@ -106,6 +106,9 @@ typedef struct gb_range_opts {
   uint32_t shard_count;   /*   s % shard_count == shard_index (0/1: all)    */
   int on_device;          /* outputs below are device pointers              */
   void* stream;           /* cudaStream_t to launch on (NULL: ctx stream)   */
+  uint32_t block_threads; /* threads per CTA of the sieve+search kernel:
+                             256, 512 or 1024 (0: 512); the CTAs per SM
+                             follow from the chunk's shared memory          */
 } gb_range_opts;
 
 typedef struct gb_range_result {
@@ -145,9 +148,11 @@ gb_status gb_verify_range(gb_ctx* ctx, uint64_t start, uint64_t limit,
  * Autotuner for gb_verify_range (no counterpart in the reference, whose
  * SEG_SIZE / P_SMALL the user picks by hand, src/goldbach.cu:560-609): times
  * gb_verify_range on the top min(2^28, count) even n of [start, limit] for
- * each candidate chunk_evens (2^18, 2^19, 2^20) and halo (2^14, 2^15, 2^16),
- * after one warm-up call, and writes the fastest into *tuned (a copy of
- * *base with chunk_evens and halo set).  The choice is cached in the context
+ * each candidate block shape (512 threads x 2 CTAs per SM, 256 x 4,
+ * 1024 x 1), chunk_evens (2^18, 2^19, 2^20) and halo (2^14, 2^15, 2^16) the
+ * shape's shared memory admits, after one warm-up call, and writes the
+ * fastest into *tuned (a copy of *base with chunk_evens, halo and
+ * block_threads set).  The choice is cached in the context
  * per range class (bit length of limit, p_small, phase2_limit): a later call
  * for the same class times nothing.  Ranges below 2^22 even n keep the
  * defaults.  Results of gb_verify_range do not depend on these knobs.
@@ -155,6 +160,7 @@ gb_status gb_verify_range(gb_ctx* ctx, uint64_t start, uint64_t limit,
 typedef struct gb_autotune_result {
   uint32_t chunk_evens;   /* chosen */
   uint32_t halo;          /* chosen */
+  uint32_t block_threads; /* chosen */
   double even_n_per_s;    /* the chosen configuration's rate on the sample */
   uint32_t candidates;    /* configurations timed by this call (0: cached) */
   uint64_t sample_evens;  /* even n per timed call */
@@ -278,8 +284,11 @@ typedef struct gb_windows_opts {
   uint64_t mr_below;      /* windows of fewer even n skip the sieve: their q
                              are tested by Miller-Rabin (the single-n
                              kernel).  0: automatic, where sieving would
-                             cost more (about pi(sqrt(top)) / 2600 n);
-                             1: never                                      */
+                             cost more (about pi(sqrt(top)) / mr_divisor
+                             n); 1: never                                  */
+  uint32_t mr_divisor;    /* the automatic split's divisor (0: 2600)        */
+  uint32_t large_ctas_per_sm; /* grid of the large-prime pass (0: 64)       */
+  uint32_t block_threads; /* as gb_range_opts.block_threads (0: 512)        */
 } gb_windows_opts;
 
 typedef struct gb_window_result {
@@ -305,6 +314,26 @@ typedef struct gb_windows_summary {
 gb_status gb_verify_windows(gb_ctx* ctx, const gb_window* w, size_t count,
                             const gb_windows_opts* opts, gb_window_result* res,
                             uint32_t* min_p_concat, gb_windows_summary* sum);
+
+/* Autotuner for gb_verify_windows (no counterpart in the reference): times
+ * the persistent pipeline on a sample of the batch (every k-th window, at
+ * most 512 windows) for each mr_divisor (1300, 2600, 5200), chunk_evens
+ * (2^19, 2^20), large-prime grid (16, 64 CTAs per SM) and block shape
+ * (512, 256 threads), after one warm-up call, and writes the fastest into
+ * *tuned (a copy of *base with those four set).  The choice is cached in the
+ * context per batch class (bit length of the largest top, bit length of the
+ * window count); a later call for the same class times nothing.  Results of
+ * gb_verify_windows do not depend on these knobs. */
+typedef struct gb_windows_tune {
+  uint32_t mr_divisor, chunk_evens, large_ctas_per_sm, block_threads; /* chosen */
+  double even_n_per_s;    /* the choice's rate on the sample */
+  uint32_t candidates;    /* configurations timed by this call (0: cached) */
+  uint32_t sample_windows;
+  int cached;
+} gb_windows_tune;
+gb_status gb_autotune_windows(gb_ctx* ctx, const gb_window* w, size_t count,
+                              const gb_windows_opts* base, gb_windows_opts* tuned,
+                              gb_windows_tune* res);
 
 /* -------------------------------------------------------------------------
  * Serving: a request loop with continuous batching.

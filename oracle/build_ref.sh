@@ -12,6 +12,11 @@
 #                       src/cpu_goldbach.cpp (main renamed)
 #   _ref/libgbref_p2.so oracle/ref_phase2_shim.cu, which includes
 #                       src/goldbach.cu (main renamed) + src/prime_bitset.cpp
+#   _ref/goldbach       src/goldbach.cu + src/prime_bitset.cpp as they are, for
+#                       sm_100a: the reference's own GPU range verifier, used
+#                       only to time it on the same B200 (its tiled sieve has
+#                       an unsynchronised shared-memory update, so it is not a
+#                       checker)
 # Flags are portable (-O3, no -march=native) so the binaries run on any
 # x86-64 host.
 set -euo pipefail
@@ -49,4 +54,7 @@ $NVCC -O3 -std=c++17 -Xcompiler -fPIC -gencode arch=compute_100a,code=sm_100a \
   -I"$S" -I"$I" -c "$HERE/ref_phase2_shim.cu" -o "$TMP/ref_phase2_shim.o"
 $NVCC -shared -cudart static -gencode arch=compute_100a,code=sm_100a -Xcompiler -fopenmp -o "$OUT/libgbref_p2.so" \
   "$TMP/ref_phase2_shim.o" "$TMP/prime_bitset.o"
+# the reference GPU verifier, unmodified (its CMake flags: -O3, OpenMP)
+$NVCC -O3 -std=c++17 -gencode arch=compute_100a,code=sm_100a -Xcompiler -fopenmp,-O3 \
+  -I"$I" "$S/goldbach.cu" "$S/prime_bitset.cpp" -o "$OUT/goldbach" -lgomp -lpthread
 echo "build_ref.sh: built $(ls "$OUT" | tr '\n' ' ')"
