@@ -514,7 +514,10 @@ def measure_serving(gb, device, rates=(1e2, 1e3, 1e4, 1e5), seconds=2.0, max_req
             span = (max(int(arr[-1]), ctx.now_ns()) - int(arr[0])) / 1e9
             out.append({"rate_rps": rate, "lane_spin_us": SERVE_SPIN_US, "requests": m,
                         "completed": sum(r["status"] == 0 for r in res),
-                        "rejected": st["rejected"], "p50_us": st["p50_us"], "p99_us": st["p99_us"],
+                        "rejected": st["rejected"], "busy": st["busy"],
+                        "range_lanes": 2, "pool_bytes": st["pool_bytes"],
+                        "pool_peak_bytes": st["pool_peak_bytes"],
+                        "p50_us": st["p50_us"], "p99_us": st["p99_us"],
                         "single_p50_us": float(np.percentile(lat_s, 50)) if lat_s.size else None,
                         "single_p99_us": float(np.percentile(lat_s, 99)) if lat_s.size else None,
                         "range_p50_us": float(np.percentile(lat_r, 50)) if lat_r.size else None,

@@ -22,7 +22,7 @@ LIB_PATH = os.path.join(HERE, "libgoldbach_b200.so")
 BIN_DIR = os.path.join(HERE, "bin")
 
 GB_OK, GB_EINVAL, GB_ENOMEM, GB_ECUDA, GB_ETIMEOUT = 0, -1, -2, -3, -4
-GB_ECANCELED, GB_ENODEV, GB_EOVERFLOW, GB_EAGAIN = -5, -6, -7, -8
+GB_ECANCELED, GB_ENODEV, GB_EOVERFLOW, GB_EAGAIN, GB_EBUSY = -5, -6, -7, -8, -9
 GB_HIST_BINS = 4096
 GB_PHASE2_LIMIT_DEFAULT = 100_000_000
 GB_WINDOWS_PERSISTENT, GB_WINDOWS_PLAIN = 0, 1
@@ -91,7 +91,8 @@ class Window(C.Structure):
 class WindowsOpts(C.Structure):
     _fields_ = [("mode", i32), ("chunk_evens", u32), ("halo", u32),
                 ("phase2_limit", u64), ("on_device", i32), ("stream", vp), ("mr_below", u64),
-                ("mr_divisor", u32), ("large_ctas_per_sm", u32), ("block_threads", u32)]
+                ("mr_divisor", u32), ("large_ctas_per_sm", u32), ("block_threads", u32),
+                ("gpu_share_pct", u32)]
 
 
 class WindowsTune(C.Structure):
@@ -129,14 +130,16 @@ class Response(C.Structure):
 class ServeOpts(C.Structure):
     _fields_ = [("max_n", u64), ("max_single_batch", u32), ("max_range_batch", u32),
                 ("range_arena_bytes", u64), ("small_range", u64), ("no_graph", u32),
-                ("spin_us", u32)]
+                ("spin_us", u32), ("range_lanes", u32), ("pool_bytes", u64),
+                ("max_pending", u64), ("max_pending_n", u64)]
 
 
 class ServeStats(C.Structure):
     _fields_ = [("submitted", u64), ("completed", u64), ("pending", u64), ("rejected", u64),
                 ("batches_single", u64), ("batches_range", u64), ("p50_us", C.c_double),
                 ("p99_us", C.c_double), ("max_us", C.c_double), ("mean_us", C.c_double),
-                ("elapsed_s", C.c_double), ("completed_per_s", C.c_double)]
+                ("elapsed_s", C.c_double), ("completed_per_s", C.c_double), ("busy", u64),
+                ("pool_bytes", u64), ("pool_peak_bytes", u64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -380,7 +383,7 @@ class Context:
         grid and block shape for this batch (timed on a sample, cached per
         batch class); the dict carries the choice and the opts to pass on."""
         w = self._windows(starts, counts)
-        base = WindowsOpts(GB_WINDOWS_PERSISTENT, 0, 0, phase2_limit, 0, None, 0, 0, 0, 0)
+        base = WindowsOpts(GB_WINDOWS_PERSISTENT, 0, 0, phase2_limit, 0, None, 0, 0, 0, 0, 0)
         tuned = WindowsOpts()
         r = WindowsTune()
         self._check(self.L.gb_autotune_windows(self._h, w, len(w), C.byref(base), C.byref(tuned),
@@ -389,7 +392,7 @@ class Context:
 
     def verify_windows(self, starts, counts, *, mode=GB_WINDOWS_PERSISTENT, chunk=0, halo=0,
                        phase2_limit=0, want_minp=False, stream=None, mr_below=0, mr_divisor=0,
-                       large_ctas_per_sm=0, block_threads=0):
+                       large_ctas_per_sm=0, block_threads=0, gpu_share_pct=0):
         counts = np.asarray(counts, dtype=np.uint64)
         w = self._windows(starts, counts)
         nw = len(w)
@@ -397,7 +400,7 @@ class Context:
         minp = np.zeros(int(counts.sum()), np.uint32) if want_minp else None
         s = WindowsSummary()
         o = WindowsOpts(mode, chunk, halo, phase2_limit, 0, stream or None, mr_below, mr_divisor,
-                        large_ctas_per_sm, block_threads)
+                        large_ctas_per_sm, block_threads, gpu_share_pct)
         self._check(self.L.gb_verify_windows(self._h, w, nw, C.byref(o), res,
                                              _ptr(minp), C.byref(s)))
         per = [{f: getattr(res[i], f) for f, _ in WindowResult._fields_} for i in range(nw)]
@@ -406,9 +409,11 @@ class Context:
     # -- serving ---------------------------------------------------------------
     def serve_start(self, max_n: int = 0, max_single_batch: int = 0, max_range_batch: int = 0,
                     range_arena_bytes: int = 0, small_range: int = 0, no_graph: bool = False,
-                    spin_us: int = 0):
+                    spin_us: int = 0, range_lanes: int = 0, pool_bytes: int = 0,
+                    max_pending: int = 0, max_pending_n: int = 0):
         o = ServeOpts(max_n, max_single_batch, max_range_batch, range_arena_bytes, small_range,
-                      1 if no_graph else 0, spin_us)
+                      1 if no_graph else 0, spin_us, range_lanes, pool_bytes, max_pending,
+                      max_pending_n)
         self._check(self.L.gb_serve_start(self._h, C.byref(o)))
 
     def submit(self, kinds, a, counts=None, arrival_ns=None) -> np.ndarray:

@@ -571,6 +571,7 @@ const char* gb_strerror(gb_status st) {
     case GB_ENODEV: return "no CUDA device";
     case GB_EOVERFLOW: return "internal queue overflow";
     case GB_EAGAIN: return "not ready";
+    case GB_EBUSY: return "busy: queued work at its bound";
     default: return "unknown error";
   }
 }

@@ -4,15 +4,20 @@
 // No counterpart in the reference, which answers one query per process
 // (`single_check <n>` re-sieves 1e8 candidates on the CPU for every query,
 // src/single_check.cu:186-198).  Here:
-//   * lane 0 (single): single n and short ranges, expanded n by n, through
-//     the single-n kernel plus a per-request reduction;
-//   * lane 1 (range): longer ranges through the windows pipeline.
-// Each lane is a host thread with its own CUDA stream, workspace and device
-// arena reserved at start, so the two lanes' batches overlap on the GPU and
-// nothing is allocated or freed while they run.  When a lane's batch
-// completes it immediately takes every request waiting for it (arrival
-// order, up to its batch size and arena), so requests that arrive while the
-// GPU is busy are admitted as soon as a lane and memory free up.
+//   * lane 0 (single, high-priority stream): single n and short ranges,
+//     expanded n by n, through the single-n kernel plus a per-request
+//     reduction, from a small arena reserved at start;
+//   * lanes 1 .. R (range): the longer ranges, from one shared queue,
+//     through the windows pipeline, with device memory split on demand from
+//     one pool: a lane forms its next batch from the waiting requests in
+//     arrival order as far as the pool's free memory allows and returns the
+//     memory when the batch completes; the kernels of a range batch fill
+//     at most 7/8 of the GPU divided among the busy range lanes.
+// Each lane is a host thread with its own CUDA stream and workspace, so the
+// lanes' batches overlap on the GPU, and nothing is allocated while they run
+// (the pool and the workspaces are reserved at start).  A request that would
+// push its lanes' queued work past max_pending / max_pending_n is answered at
+// once with GB_EBUSY.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -20,6 +25,7 @@
 #include <cstring>
 #include <deque>
 #include <thread>
+#include <map>
 #include <unordered_map>
 
 #include "gb_ctx.h"
@@ -35,11 +41,63 @@ struct Pending {
 
 struct Lane {
   Workspace ws;
-  Arena arena;
+  Arena arena;             // the single lane's fixed buffers
   void* arena_mem = nullptr;
   cudaStream_t stream = nullptr;
   std::thread th;
   uint64_t batches = 0;
+  bool busy = false;       // a range lane with a batch on the GPU
+};
+
+// First-fit allocator over one device allocation (host-side bookkeeping,
+// under the server mutex): the range lanes' batches take their memory from
+// it and give it back when they complete.
+struct Pool {
+  char* base = nullptr;
+  uint64_t cap = 0, used = 0, peak = 0;
+  std::map<uint64_t, uint64_t> free_;  // offset -> bytes, coalesced
+  void init(void* p, uint64_t bytes) {
+    base = (char*)p;
+    cap = bytes & ~255ull;
+    free_.clear();
+    if (cap) free_[0] = cap;
+  }
+  uint64_t largest() const {
+    uint64_t m = 0;
+    for (const auto& f : free_) m = std::max(m, f.second);
+    return m;
+  }
+  bool alloc(uint64_t bytes, uint64_t* off) {
+    bytes = (bytes + 255) & ~255ull;
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second < bytes) continue;
+      *off = it->first;
+      const uint64_t rest = it->second - bytes;
+      free_.erase(it);
+      if (rest) free_[*off + bytes] = rest;
+      used += bytes;
+      peak = std::max(peak, used);
+      return true;
+    }
+    return false;
+  }
+  void release(uint64_t off, uint64_t bytes) {
+    bytes = (bytes + 255) & ~255ull;
+    used -= bytes;
+    auto it = free_.emplace(off, bytes).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
 };
 
 uint64_t now_ns() {
@@ -49,6 +107,8 @@ uint64_t now_ns() {
 }
 
 constexpr uint32_t kSingleReqCap = 1u << 16;  // requests per single-lane batch
+constexpr int kMaxRangeLanes = 8;
+constexpr uint64_t kBatchSlack = 64 << 10;  // per-batch alignment of the pool block
 
 }  // namespace
 
@@ -57,30 +117,35 @@ struct gb_server {
   gb_serve_opts o{};
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
-  std::deque<Pending> q[2];
-  // requests queued per lane and the stop request, readable without the
+  std::deque<Pending> q[2];  // 0: single lane, 1: the range lanes
+  // requests queued per queue and the stop request, readable without the
   // mutex by a lane that polls (opts.spin_us)
   std::atomic<uint64_t> queued[2];
   std::atomic<bool> stopping{false};
   std::unordered_map<uint64_t, gb_response> done;
   uint64_t next_ticket = 1;
   bool stop = false;
-  Lane lane[2];
+  int nlanes = 0;            // 1 + range lanes
+  Lane lane[1 + kMaxRangeLanes];
+  Pool pool;                 // range lanes' device memory
+  void* pool_mem = nullptr;
+  uint64_t queued_n = 0;     // even n waiting in the range queue
+  int busy_range = 0;        // range lanes with a batch on the GPU
   // single-lane pinned staging
   uint64_t *h_n = nullptr, *h_p = nullptr, *h_off = nullptr;
   unsigned long long* h_agg = nullptr;
   bool single_graph = false;  // the single lane runs its small batches as a graph
   // stats
   std::vector<double> lat;
-  uint64_t submitted = 0, completed = 0, rejected = 0, t0 = 0;
+  uint64_t submitted = 0, completed = 0, rejected = 0, busy = 0, t0 = 0;
 };
 
 namespace {
 
-// bytes the range lane's windows call takes from its arena for a batch
+// Device bytes of a range request in a range-lane batch (its windows call).
 uint64_t range_bytes(const gb_request& r) {
-  const uint64_t wbits = ((32768 / 2 + r.count + 64 + 128) + 127) / 128 * 128;
-  return wbits / 8 + 112;  // + descriptor, (g0, bits) record, offsets, results
+  gb_windows_opts o{};
+  return windows_request_bytes(gb_window{r.a, r.count}, o);
 }
 
 void finish(gb_server* S, const Pending& p, gb_response& resp, uint64_t t_done) {
@@ -286,49 +351,88 @@ void single_lane(gb_server* S) {
   }
 }
 
-void range_lane(gb_server* S) {
-  Lane& L = S->lane[1];
+// Range lane ln: batches from the shared range queue, memory from the pool.
+void range_lane(gb_server* S, int ln) {
+  Lane& L = S->lane[ln];
   gb_ctx* c = S->c;
   std::vector<Pending> take;
   std::vector<gb_window> win;
   std::vector<gb_window_result> res;
   for (;;) {
     take.clear();
+    uint64_t off = 0, bytes = 0;
+    bool nomem = false;
+    int sharing = 1;
     {
       std::unique_lock<std::mutex> lk(S->mu);
       lk.unlock();
       poll_queue(S, 1);
       lk.lock();
-      S->cv_work.wait(lk, [&] { return S->stop || !S->q[1].empty(); });
-      if (S->q[1].empty()) break;
-      uint64_t bytes = 64 << 10;
-      while (!S->q[1].empty() && take.size() < S->o.max_range_batch) {
-        const Pending& f = S->q[1].front();
-        const uint64_t b = range_bytes(f.r);
-        if (!take.empty() && bytes + b > L.arena.cap) break;
-        take.push_back(f);
-        bytes += b;
+      for (;;) {  // until the front request fits the pool (or stop)
+        if (!S->q[1].empty()) {
+          const uint64_t need = range_bytes(S->q[1].front().r) + kBatchSlack;
+          if (need <= S->pool.largest()) break;
+          if (S->busy_range == 0) {  // all memory free and still too big
+            nomem = true;
+            break;
+          }
+        } else if (S->stop) {
+          break;
+        }
+        S->cv_work.wait(lk);
+      }
+      if (S->q[1].empty()) break;  // stop requested and drained
+      if (nomem) {
+        take.push_back(S->q[1].front());
         S->q[1].pop_front();
         S->queued[1].fetch_sub(1, std::memory_order_relaxed);
+        S->queued_n -= take[0].r.count;
+      } else {
+        const uint64_t avail = S->pool.largest();
+        bytes = kBatchSlack;
+        while (!S->q[1].empty() && take.size() < S->o.max_range_batch) {
+          const Pending& f = S->q[1].front();
+          const uint64_t b = range_bytes(f.r);
+          if (bytes + b > avail) break;
+          take.push_back(f);
+          bytes += b;
+          S->queued_n -= f.r.count;
+          S->q[1].pop_front();
+          S->queued[1].fetch_sub(1, std::memory_order_relaxed);
+        }
+        S->pool.alloc(bytes, &off);  // bytes <= the largest free block
+        L.busy = true;
+        sharing = ++S->busy_range;
       }
     }
-    win.resize(take.size());
-    res.assign(take.size(), gb_window_result{});
-    for (size_t i = 0; i < take.size(); ++i) win[i] = gb_window{take[i].r.a, take[i].r.count};
-    gb_windows_opts o{};
-    o.mode = GB_WINDOWS_PERSISTENT;
-    o.stream = L.stream;
-    gb_windows_summary sum{};
-    L.arena.used = 0;
-    const gb_status st = windows_impl(c, L.ws, &L.arena, win.data(), win.size(), &o, res.data(),
-                                      nullptr, &sum);
-    L.arena.used = 0;
-    const uint64_t t_done = now_ns();
     const uint32_t batch = (uint32_t)L.batches++;
+    gb_status st = GB_ENOMEM;
+    res.assign(take.size(), gb_window_result{});
+    if (!nomem) {
+      win.resize(take.size());
+      for (size_t i = 0; i < take.size(); ++i) win[i] = gb_window{take[i].r.a, take[i].r.count};
+      gb_windows_opts o{};
+      o.mode = GB_WINDOWS_PERSISTENT;
+      o.stream = L.stream;
+      o.gpu_share_pct = (uint32_t)std::max(1, 7 * 100 / 8 / sharing);
+      Arena arena;
+      arena.base = S->pool.base + off;
+      arena.cap = bytes;
+      gb_windows_summary sum{};
+      st = windows_impl(c, L.ws, &arena, win.data(), win.size(), &o, res.data(), nullptr, &sum);
+      {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->pool.release(off, bytes);
+        L.busy = false;
+        --S->busy_range;
+      }
+      S->cv_work.notify_all();  // memory freed: a waiting lane may fit its batch now
+    }
+    const uint64_t t_done = now_ns();
     for (size_t i = 0; i < take.size(); ++i) {
       gb_response resp{};
       resp.kind = GB_REQ_RANGE;
-      resp.lane = 1;
+      resp.lane = (uint32_t)ln;
       resp.batch = batch;
       resp.status = st;
       if (st == GB_OK) {
@@ -352,6 +456,7 @@ void free_server(gb_server* S) {
     ws_free(c, L.ws);
     dev_free(c, L.arena_mem);
   }
+  dev_free(c, S->pool_mem);
   if (S->h_n) cudaFreeHost(S->h_n);
   if (S->h_p) cudaFreeHost(S->h_p);
   if (S->h_off) cudaFreeHost(S->h_off);
@@ -378,30 +483,64 @@ gb_status gb_serve_start(gb_ctx* c, const gb_serve_opts* opts) {
   if (!S->o.max_n) S->o.max_n = ~0ull;
   if (!S->o.max_single_batch) S->o.max_single_batch = 1u << 18;
   if (!S->o.max_range_batch) S->o.max_range_batch = 4096;
-  if (!S->o.range_arena_bytes) S->o.range_arena_bytes = 4ull << 30;
   if (!S->o.small_range) S->o.small_range = 1u << 15;
   if (S->o.small_range > S->o.max_single_batch) S->o.small_range = S->o.max_single_batch;
-  // resident tables for every n served: sieving primes to sqrt(max_n) and
-  // the candidate primes; frozen while the lanes run
-  gb_status st = ensure_primes(c, c->ws, std::max<uint64_t>(isqrt_u64(S->o.max_n) + 2,
-                                                            GB_PHASE2_LIMIT_DEFAULT));
+  if (!S->o.range_lanes) S->o.range_lanes = 2;
+  if (!S->o.max_pending) S->o.max_pending = 1u << 16;
+  if (!S->o.max_pending_n) S->o.max_pending_n = 1ull << 31;
   auto bail = [&](gb_status x) {
     c->err = c->ws.err;
     free_server(S);
     return x;
   };
+  if (S->o.range_lanes > kMaxRangeLanes) {
+    c->ws.err = "range_lanes must be <= 8";
+    return bail(GB_EINVAL);
+  }
+  S->nlanes = 1 + (int)S->o.range_lanes;
+  // resident tables for every n served: sieving primes to sqrt(max_n) and
+  // the candidate primes; frozen while the lanes run
+  gb_status st = ensure_primes(c, c->ws, std::max<uint64_t>(isqrt_u64(S->o.max_n) + 2,
+                                                            GB_PHASE2_LIMIT_DEFAULT));
   if (st != GB_OK) return bail(st);
   const uint64_t cap = S->o.max_single_batch;
   const uint64_t single_bytes = cap * 24 + (kSingleReqCap + 1) * 8 + kSingleReqCap * 32 + 4096;
-  const uint64_t arena_bytes[2] = {single_bytes, S->o.range_arena_bytes};
-  for (int i = 0; i < 2; ++i) {
+  int lo_prio = 0, hi_prio = 0;
+  cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
+  // survivor lists of the chunk kernel at its default shape on the full GPU
+  const size_t surv_bytes = (size_t)c->sm_count * 2 * 6 * range6_words(32768, 1u << 20) * sizeof(uint2);
+  for (int i = 0; i < S->nlanes; ++i) {
     Lane& L = S->lane[i];
     if ((st = ws_init(c, L.ws, 1u << 16)) != GB_OK) return bail(st);
-    if ((st = dev_alloc(c, &L.arena_mem, arena_bytes[i], &c->ws.err)) != GB_OK) return bail(st);
-    L.arena.base = (char*)L.arena_mem;
-    L.arena.cap = arena_bytes[i];
-    if (cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking) != cudaSuccess) return bail(GB_ECUDA);
+    if (i == 0) {
+      if ((st = dev_alloc(c, &L.arena_mem, single_bytes, &c->ws.err)) != GB_OK) return bail(st);
+      L.arena.base = (char*)L.arena_mem;
+      L.arena.cap = single_bytes;
+    } else {
+      void* p = nullptr;
+      if ((st = ws_scratch(c, L.ws, surv_bytes, &p)) != GB_OK) return bail(st);
+    }
+    // the single lane's short batches go ahead of the range lanes' blocks
+    if (cudaStreamCreateWithPriority(&L.stream, cudaStreamNonBlocking, i == 0 ? hi_prio : lo_prio) !=
+        cudaSuccess)
+      return bail(GB_ECUDA);
   }
+  // the range lanes' pool: as asked, else half of what the device has free
+  // now, within the context's budget
+  uint64_t pool = S->o.pool_bytes ? S->o.pool_bytes : S->o.range_arena_bytes;
+  if (!pool) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return bail(GB_ECUDA);
+    pool = fr / 2;
+    const uint64_t left = c->budget > c->held ? c->budget - c->held : 0;
+    pool = std::min<uint64_t>(pool, left > (64ull << 20) ? left - (64ull << 20) : 0);
+  }
+  if (pool < (256ull << 10)) {
+    c->ws.err = "no device memory left for the serving pool";
+    return bail(GB_ENOMEM);
+  }
+  if ((st = dev_alloc(c, &S->pool_mem, pool, &c->ws.err)) != GB_OK) return bail(st);
+  S->pool.init(S->pool_mem, pool);
   if (cudaHostAlloc((void**)&S->h_n, cap * 8, cudaHostAllocDefault) != cudaSuccess ||
       cudaHostAlloc((void**)&S->h_p, cap * 8, cudaHostAllocDefault) != cudaSuccess ||
       cudaHostAlloc((void**)&S->h_off, (kSingleReqCap + 1) * 8, cudaHostAllocDefault) != cudaSuccess ||
@@ -413,10 +552,11 @@ gb_status gb_serve_start(gb_ctx* c, const gb_serve_opts* opts) {
     cudaSetDevice(S->c->device);
     single_lane(S);
   });
-  S->lane[1].th = std::thread([S] {
-    cudaSetDevice(S->c->device);
-    range_lane(S);
-  });
+  for (int i = 1; i < S->nlanes; ++i)
+    S->lane[i].th = std::thread([S, i] {
+      cudaSetDevice(S->c->device);
+      range_lane(S, i);
+    });
   return GB_OK;
 }
 
@@ -436,14 +576,19 @@ gb_status gb_submit(gb_ctx* c, const gb_request* reqs, size_t count, uint64_t* t
     bool ok = r.a >= 4 && !(r.a & 1) && r.a <= S->o.max_n;
     if (r.kind == GB_REQ_RANGE) {
       const uint64_t last = r.a + 2 * (r.count - 1);
-      ok = ok && r.count >= 1 && r.count <= (1ull << 40) && last >= r.a && last <= S->o.max_n;
+      ok = ok && r.count >= 1 && r.count <= GB_WINDOW_MAX_COUNT && last >= r.a && last <= S->o.max_n;
     } else if (r.kind != GB_REQ_SINGLE) {
       ok = false;
     }
+    const int ln = (r.kind == GB_REQ_SINGLE || r.count <= S->o.small_range) ? 0 : 1;
     gb_status bad = ok ? GB_OK : GB_EINVAL;
-    if (ok && r.kind == GB_REQ_RANGE && r.count > S->o.small_range &&
-        range_bytes(r) + (64 << 10) > S->lane[1].arena.cap)
-      bad = GB_ENOMEM;  // would never fit the range lane's memory
+    if (bad == GB_OK && ln == 1 && range_bytes(r) + kBatchSlack > S->pool.cap)
+      bad = GB_ENOMEM;  // would never fit the range lanes' memory
+    // backpressure: the queue of the request's lanes is at its bound (an
+    // empty queue always takes the request)
+    if (bad == GB_OK && ln == 0 && S->q[0].size() >= S->o.max_pending) bad = GB_EBUSY;
+    if (bad == GB_OK && ln == 1 && !S->q[1].empty() && S->queued_n + r.count > S->o.max_pending_n)
+      bad = GB_EBUSY;
     if (bad != GB_OK) {
       gb_response resp{};
       resp.status = bad;
@@ -451,9 +596,10 @@ gb_status gb_submit(gb_ctx* c, const gb_request* reqs, size_t count, uint64_t* t
       S->done[p.ticket] = resp;
       S->completed++;
       S->rejected++;
+      if (bad == GB_EBUSY) S->busy++;
       continue;
     }
-    const int ln = (r.kind == GB_REQ_SINGLE || r.count <= S->o.small_range) ? 0 : 1;
+    if (ln == 1) S->queued_n += r.count;
     S->q[ln].push_back(p);
     S->queued[ln].fetch_add(1, std::memory_order_release);
   }
@@ -495,7 +641,10 @@ gb_status gb_serve_stats_get(gb_ctx* c, gb_serve_stats* out, int reset) {
   out->pending = S->q[0].size() + S->q[1].size();
   out->rejected = S->rejected;
   out->batches_single = S->lane[0].batches;
-  out->batches_range = S->lane[1].batches;
+  for (int i = 1; i < S->nlanes; ++i) out->batches_range += S->lane[i].batches;
+  out->busy = S->busy;
+  out->pool_bytes = S->pool.cap;
+  out->pool_peak_bytes = S->pool.peak;
   out->elapsed_s = (now_ns() - S->t0) / 1e9;
   if (!S->lat.empty()) {
     std::vector<double> v = S->lat;

@@ -57,6 +57,8 @@ static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, cons
   const uint64_t p_lim = o.phase2_limit ? o.phase2_limit : GB_PHASE2_LIMIT_DEFAULT;
   if (p_lim > GB_P_SMALL_MAX) return fail(ws, GB_EINVAL, "phase2_limit must be <= 4e9");
   const uint64_t large_per_sm = o.large_ctas_per_sm ? o.large_ctas_per_sm : kLargeBlocksPerSM;
+  if (o.gpu_share_pct > 100) return fail(ws, GB_EINVAL, "gpu_share_pct must be <= 100");
+  const uint64_t share = o.gpu_share_pct ? o.gpu_share_pct : 100;
   uint64_t total_n = 0, q_max = 0;
   for (size_t i = 0; i < count; ++i) {
     if (w[i].start < 4 || (w[i].start & 1) || w[i].count == 0)
@@ -180,7 +182,8 @@ static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, cons
   const int sm = c->sm_count;
   int bps = range_max_blocks_per_sm(a);
   if (bps < 1) bps = 1;
-  const uint64_t grid_max = (uint64_t)sm * bps;
+  // CTAs the chunk kernel may keep resident: its share of the GPU
+  const uint64_t grid_max = std::max<uint64_t>(1, (uint64_t)sm * bps * share / 100);
   a.surv_cap = nbw;
   {
     void* p = nullptr;
@@ -188,7 +191,12 @@ static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, cons
     a.surv = (uint2*)p;
   }
   const uint64_t np = la.k1 - la.k0;
-  const int gl = (int)std::max<uint64_t>(1, std::min<uint64_t>((np + 255) / 256, (uint64_t)sm * large_per_sm));
+  // the large-prime pass: kLargeResident CTAs of 256 threads fit an SM at
+  // once; a share below 100% keeps its grid within that share of the slots
+  constexpr uint64_t kLargeResident = 5;
+  uint64_t gl_cap = (uint64_t)sm * large_per_sm;
+  if (share < 100) gl_cap = std::min<uint64_t>(gl_cap, std::max<uint64_t>(1, sm * kLargeResident * share / 100));
+  const int gl = (int)std::max<uint64_t>(1, std::min<uint64_t>((np + 255) / 256, gl_cap));
 
   cudaStream_t s = o.stream ? (cudaStream_t)o.stream : c->stream;
   cudaError_t e = cudaSuccess;
@@ -335,7 +343,9 @@ static gb_status windows_mr_impl(gb_ctx* c, Workspace& ws, Arena* arena, const g
     a.p_out = (uint64_t*)d_p + b;
     a.q_out = (uint64_t*)d_q + b;
     chk(cudaMemsetAsync(ws.ctr, 0, 4 * 8, s));
-    const uint64_t grid = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)c->sm_count * 6, (n + 7) / 8));
+    const uint64_t share = o.gpu_share_pct ? o.gpu_share_pct : 100;
+    const uint64_t gcap = std::max<uint64_t>(1, (uint64_t)c->sm_count * 6 * share / 100);
+    const uint64_t grid = std::max<uint64_t>(1, std::min<uint64_t>(gcap, (n + 7) / 8));
     chk(launch_single(a, (int)grid, s));
     ++launches;
   }
@@ -448,6 +458,26 @@ gb_status windows_impl(gb_ctx* c, Workspace& ws, Arena* arena, const gb_window* 
     sum->search_ms = sb.search_ms;
   }
   return GB_OK;
+}
+
+// Upper bound of the device bytes one window takes from a caller's arena in
+// windows_impl: its share of the sieve path's buffers (descriptor, record,
+// offsets, results, class masks) or, when it is narrow enough for the
+// Miller-Rabin path, of that path's (its n, p, q and a reduction record);
+// arena alignment included.  Used by serving to admit batches by memory.
+uint64_t windows_request_bytes(const gb_window& w, const gb_windows_opts& o) {
+  const uint64_t H = o.halo ? o.halo : 32768u;
+  const uint64_t last = w.start + 2 * (w.count - 1);
+  uint64_t lim = o.mr_below;
+  if (!lim) {
+    const double r = std::sqrt((double)last);
+    const double div = o.mr_divisor ? (double)o.mr_divisor : kMrBelowDivisor;
+    lim = r > 1e4 ? (uint64_t)(1.1 * r / std::log(r) / div) : 0;
+  }
+  const uint64_t fixed = sizeof(WinDesc6) + sizeof(WinLarge) + 24 + 4 + 16 + 16 + 4 * 256;
+  if (w.count < lim) return fixed + w.count * 24 + 64 + 4 * 256;
+  const uint64_t lwords = (w.count / 3 + H / 6 + 96) / 32 + 16;
+  return fixed + 2 * lwords * 4;
 }
 
 // Autotuner of the windows pipeline: the persistent mode on a sample of the

@@ -42,6 +42,7 @@ typedef int gb_status;
 #define GB_ENODEV (-6)    /* no CUDA device */
 #define GB_EOVERFLOW (-7) /* an internal queue would overflow */
 #define GB_EAGAIN (-8)    /* serving: result not ready yet */
+#define GB_EBUSY (-9)     /* serving: refused, the queued work is at its bound */
 
 /* Minimal-p histogram: bin k counts n whose minimal p is the k-th prime
  * (2 -> bin 0, 3 -> 1, 5 -> 2, ...); minimal p of index >= GB_HIST_BINS-1
@@ -289,6 +290,9 @@ typedef struct gb_windows_opts {
   uint32_t mr_divisor;    /* the automatic split's divisor (0: 2600)        */
   uint32_t large_ctas_per_sm; /* grid of the large-prime pass (0: 64)       */
   uint32_t block_threads; /* as gb_range_opts.block_threads (0: 512)        */
+  uint32_t gpu_share_pct; /* each kernel of the call fills at most this
+                             percentage of the GPU's resident CTA slots
+                             (0: 100), leaving the rest to concurrent work */
 } gb_windows_opts;
 
 typedef struct gb_window_result {
@@ -340,14 +344,24 @@ gb_status gb_autotune_windows(gb_ctx* ctx, const gb_window* w, size_t count,
  *
  * The reference serves one query per process (`single_check <n>`, or a
  * `goldbach --start=A L` run).  Here requests are submitted from any thread
- * and complete independently.  Two lanes run concurrently on their own
- * streams over the context's resident tables: the single lane runs single
- * n and short ranges (n by n) through the single-n kernel; the range lane
- * runs the other ranges through the windows pipeline.  A lane takes every
- * request that is waiting when its previous batch finishes, in arrival
- * order, as far as its batch size and its device memory (an arena reserved
- * at start) allow; requests that arrive meanwhile join the lane's next
- * batch.  Each result depends only on its own request.
+ * and complete independently.  Lanes run concurrently on their own streams
+ * over the context's resident tables:
+ *   - the single lane (lane 0, a high-priority stream) runs single n and
+ *     short ranges (n by n) through the single-n kernel;
+ *   - the range lanes (lanes 1 .. range_lanes) take the other ranges from
+ *     one queue through the windows pipeline; a lane's kernels fill at most
+ *     its share of the GPU (7/8 of it split among the busy range lanes), so
+ *     the single lane always finds free SMs and a wide range never holds up
+ *     the narrow ones behind it.
+ * Device memory for the range batches is one pool reserved at start (from
+ * the device's free memory); a range lane takes, when its previous batch
+ * completes, every waiting request in arrival order as far as its batch
+ * size and the pool's free memory allow, and gives the memory back when the
+ * batch completes -- a request that does not fit yet waits in the queue.
+ * Requests that arrive meanwhile join the next batches.  Backpressure: a
+ * request that would bring the queued (not yet started) work of its lanes
+ * above max_pending / max_pending_n completes at once with GB_EBUSY.  Each
+ * result depends only on its own request.
  * ---------------------------------------------------------------------- */
 #define GB_REQ_SINGLE 0 /* n = a (even, >= 4)                       */
 #define GB_REQ_RANGE 1  /* every even n in [a, a + 2*(count-1)]      */
@@ -368,7 +382,7 @@ typedef struct gb_response {
   uint64_t max_minp;
   uint64_t minp_sum;  /* sum of minimal p over the request                */
   double latency_us;  /* arrival to completion                            */
-  uint32_t lane;      /* 0: single lane, 1: range lane                    */
+  uint32_t lane;      /* 0: single lane, 1 .. range_lanes: a range lane   */
   uint32_t batch;     /* the lane batch that served it                    */
 } gb_response;
 
@@ -383,14 +397,23 @@ typedef struct gb_serve_opts {
   uint32_t spin_us;            /* a lane out of work polls its queue this long
                                   before it blocks (0: blocks at once; polling
                                   keeps a host core busy per lane)           */
+  uint32_t range_lanes;        /* range lanes (0: 2)                           */
+  uint64_t pool_bytes;         /* device memory pool of the range lanes (0:
+                                  range_arena_bytes if set, else half of the
+                                  free device memory at start, within the
+                                  context's budget)                          */
+  uint64_t max_pending;        /* queued single-lane requests (0: 2^16)        */
+  uint64_t max_pending_n;      /* queued even n of the range lanes (0: 2^31)   */
 } gb_serve_opts;
 
 typedef struct gb_serve_stats {
-  uint64_t submitted, completed, pending, rejected;
+  uint64_t submitted, completed, pending, rejected; /* rejected: invalid + busy */
   uint64_t batches_single, batches_range;
   double p50_us, p99_us, max_us, mean_us; /* latency of completed requests */
   double elapsed_s;                       /* since start or last reset       */
   double completed_per_s;
+  uint64_t busy;                          /* refused with GB_EBUSY           */
+  uint64_t pool_bytes, pool_peak_bytes;   /* range pool: size, peak in use   */
 } gb_serve_stats;
 
 /* Measured peaks for the roofline of the integer kernels: 32-bit ALU

@@ -43,7 +43,7 @@ def test_mixed_stream_matches_requests_run_alone(gbmod):
         assert st["completed"] == st["submitted"] == len(reqs)
         assert st["rejected"] == 0 and st["p99_us"] >= st["p50_us"] > 0
         lanes = {g["lane"] for g in got}
-        assert lanes == {0, 1}
+        assert 0 in lanes and lanes - {0} and lanes <= {0, 1, 2}
         for (kind, a, count), g in zip(reqs, got):
             assert g["status"] == 0
             want = _alone(ctx, kind, a, count)
@@ -77,7 +77,7 @@ def test_high_offsets_match_the_oracle(gbmod, oracle):
                  for _ in range(12)]
         k, a, c = zip(*reqs)
         got = [ctx.wait(t, 120000) for t in ctx.submit(k, a, c)]
-        assert {g["lane"] for g in got} == {0, 1}
+        assert 0 in {g["lane"] for g in got} and {g["lane"] for g in got} - {0}
         for (kind, a0, count), g in zip(reqs, got):
             ns = np.array([a0 + 2 * j for j in range(count)], np.uint64)
             m = oracle.single_minp(ns, p_limit=10**8)
@@ -113,3 +113,36 @@ def test_graph_and_stream_launches_agree(gbmod):
         p, _, _ = ctx.check_single(np.array(a, np.uint64))
     assert out[(False, 0)] == out[(True, 0)] == out[(False, 2000)]
     assert [o[0] for o in out[(False, 0)][:len(a)]] == [int(x) for x in p]
+
+
+def test_backpressure_and_a_small_pool(gbmod):
+    """A pool of 256 KB holds only a few ranges at a time: the rest wait in the
+    queue for memory (deferred, not failed).  With max_pending_n at 2^21 a
+    burst of wide ranges is partly refused with GB_EBUSY at once; everything
+    admitted completes with the result it has alone; three range lanes."""
+    with gbmod.Context(0, max_n=10**13) as ctx:
+        ctx.serve_start(max_n=10**13, small_range=2000, range_lanes=3, pool_bytes=256 << 10,
+                        max_pending_n=1 << 21)
+        rng = np.random.default_rng(9)
+        reqs = [(1, int(rng.integers(2, 5 * 10**12)) * 2, int(rng.integers(100000, 400000)))
+                for _ in range(40)]
+        reqs += [(0, int(rng.integers(2, 5 * 10**12)) * 2, 1) for _ in range(50)]
+        k, a, c = zip(*reqs)
+        got = [ctx.wait(t, 120000) for t in ctx.submit(k, a, c)]
+        st = ctx.serve_stats()
+        busy = [g for g in got if g["status"] == gbmod.GB_EBUSY]
+        assert busy and st["busy"] == len(busy) and st["rejected"] == len(busy)
+        assert all(g["kind"] == 1 for g in busy)  # the single lane's queue was never full
+        assert st["pool_bytes"] == 256 << 10 and 0 < st["pool_peak_bytes"] <= 256 << 10
+        assert st["batches_range"] >= 3  # the admitted ranges did not fit one batch
+        done = [(r, g) for r, g in zip(reqs, got) if g["status"] == 0]
+        assert len(done) + len(busy) == len(reqs)
+        assert {g["lane"] for r, g in done if r[0] == 1} <= {1, 2, 3}
+        for (kind, a0, count), g in done:
+            want = _alone(ctx, kind, a0, count)
+            for key, v in want.items():
+                assert g[key] == v, (kind, a0, count, key)
+        # the queue drains: a later request is admitted again
+        r = ctx.wait(ctx.submit([1], [10**12], [300000])[0], 120000)
+        assert r["status"] == 0
+        ctx.serve_stop()
