@@ -191,12 +191,11 @@ static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, cons
     a.surv = (uint2*)p;
   }
   const uint64_t np = la.k1 - la.k0;
-  // the large-prime pass: kLargeResident CTAs of 256 threads fit an SM at
-  // once; a share below 100% keeps its grid within that share of the slots
-  constexpr uint64_t kLargeResident = 5;
-  uint64_t gl_cap = (uint64_t)sm * large_per_sm;
-  if (share < 100) gl_cap = std::min<uint64_t>(gl_cap, std::max<uint64_t>(1, sm * kLargeResident * share / 100));
-  const int gl = (int)std::max<uint64_t>(1, std::min<uint64_t>((np + 255) / 256, gl_cap));
+  // the large-prime pass is not capped by the share: its CTAs are short
+  // (a few primes each, grid-stride) and free their slots as they finish,
+  // where higher-priority work takes them; a capped grid left it with too
+  // few warps per SM to hide its loads
+  const int gl = (int)std::max<uint64_t>(1, std::min<uint64_t>((np + 255) / 256, (uint64_t)sm * large_per_sm));
 
   cudaStream_t s = o.stream ? (cudaStream_t)o.stream : c->stream;
   cudaError_t e = cudaSuccess;

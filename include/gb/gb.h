@@ -290,9 +290,11 @@ typedef struct gb_windows_opts {
   uint32_t mr_divisor;    /* the automatic split's divisor (0: 2600)        */
   uint32_t large_ctas_per_sm; /* grid of the large-prime pass (0: 64)       */
   uint32_t block_threads; /* as gb_range_opts.block_threads (0: 512)        */
-  uint32_t gpu_share_pct; /* each kernel of the call fills at most this
-                             percentage of the GPU's resident CTA slots
-                             (0: 100), leaving the rest to concurrent work */
+  uint32_t gpu_share_pct; /* the persistent kernels of the call (chunk
+                             sieve + search, Miller-Rabin path) fill at most
+                             this percentage of the GPU's resident CTA
+                             slots (0: 100), leaving the rest to concurrent
+                             work                                          */
 } gb_windows_opts;
 
 typedef struct gb_window_result {

@@ -117,15 +117,15 @@ def test_graph_and_stream_launches_agree(gbmod):
 
 def test_backpressure_and_a_small_pool(gbmod):
     """A pool of 256 KB holds only a few ranges at a time: the rest wait in the
-    queue for memory (deferred, not failed).  With max_pending_n at 2^21 a
+    queue for memory (deferred, not failed).  With max_pending_n at 2^23 a
     burst of wide ranges is partly refused with GB_EBUSY at once; everything
     admitted completes with the result it has alone; three range lanes."""
     with gbmod.Context(0, max_n=10**13) as ctx:
         ctx.serve_start(max_n=10**13, small_range=2000, range_lanes=3, pool_bytes=256 << 10,
-                        max_pending_n=1 << 21)
+                        max_pending_n=1 << 23)
         rng = np.random.default_rng(9)
         reqs = [(1, int(rng.integers(2, 5 * 10**12)) * 2, int(rng.integers(100000, 400000)))
-                for _ in range(40)]
+                for _ in range(60)]
         reqs += [(0, int(rng.integers(2, 5 * 10**12)) * 2, 1) for _ in range(50)]
         k, a, c = zip(*reqs)
         got = [ctx.wait(t, 120000) for t in ctx.submit(k, a, c)]
