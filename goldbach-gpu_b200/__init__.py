@@ -84,6 +84,13 @@ class SingleResult(C.Structure):
                 ("device_ms", C.c_double)]
 
 
+class BigResult(C.Structure):
+    _fields_ = [("candidates", u64), ("mr_tests", u64), ("device_ms", C.c_double)]
+
+
+GB_BIG_MAX_LIMBS = 128
+
+
 class Window(C.Structure):
     _fields_ = [("start", u64), ("count", u64)]
 
@@ -177,6 +184,7 @@ def load(path: str = LIB_PATH):
                                       P(WindowsTune)]),
         "gb_primes_upto": (i32, [vp, u64, vp, u64, P(u64)]),
         "gb_is_prime_batch": (i32, [vp, vp, C.c_size_t, vp, i32, vp]),
+        "gb_check_big": (i32, [vp, vp, u32, u64, P(u64), vp, P(BigResult)]),
         "gb_check_single_batch": (i32, [vp, vp, C.c_size_t, vp, vp, P(SingleOpts), P(SingleResult)]),
         "gb_verify_windows": (i32, [vp, P(Window), C.c_size_t, P(WindowsOpts), P(WindowResult),
                                     vp, P(WindowsSummary)]),
@@ -366,6 +374,20 @@ class Context:
         self._check(self.L.gb_check_single_batch(self._h, ns.ctypes.data, len(ns), p.ctypes.data,
                                                  q.ctypes.data, C.byref(o), C.byref(r)))
         return p, q, r
+
+    def check_big(self, n: int, p_limit: int = 0):
+        """gb_check_big: the minimal p <= p_limit with n - p a probable prime
+        (12-base strong test; deterministic below 3.3e24) for an even n of up
+        to 4096 bits.  Returns (p, q, result dict); p = q = 0: none."""
+        nl = max(1, (n.bit_length() + 31) // 32)
+        limbs = np.array([(n >> (32 * i)) & 0xFFFFFFFF for i in range(nl)], dtype=np.uint32)
+        q = np.zeros(nl, np.uint32)
+        p = u64()
+        r = BigResult()
+        self._check(self.L.gb_check_big(self._h, limbs.ctypes.data, nl, p_limit, C.byref(p),
+                                        q.ctypes.data, C.byref(r)))
+        qv = sum(int(x) << (32 * i) for i, x in enumerate(q))
+        return p.value, qv, {f: getattr(r, f) for f, _ in BigResult._fields_}
 
     # -- windows -------------------------------------------------------------
     @staticmethod

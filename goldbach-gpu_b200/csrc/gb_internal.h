@@ -160,6 +160,26 @@ cudaError_t launch_win_large(const WinLargeArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_win_pairs(const WinDesc6* win, uint32_t nwin, const uint32_t* primes, uint64_t nprimes,
                              uint32_t k0, unsigned long long* pairs, cudaStream_t s);
 
+// kernels/big.cu: partitions of n beyond 2^64.  One batch of candidates
+// primes[k0 .. k0 + kcount): the filter appends the indices (from k0) whose
+// q = n - p no trial prime divides; the test lowers *best to the smallest
+// index whose q passes the 12-base strong probable-prime test.
+struct BigArgs {
+  const uint32_t* n;        // n in `limbs` little-endian 32-bit limbs (zero-padded)
+  uint32_t limbs;           // 4, 8, 16, 32, 64 or 128
+  const uint32_t* primes;
+  uint64_t p_lim;           // candidates p <= p_lim
+  const uint32_t* trial;    // trial primes r
+  const uint32_t* nmod;     // n mod r
+  uint32_t ntrial;
+  uint32_t* surv;           // survivors (candidate index from k0)
+  uint32_t* nsurv;
+  uint32_t* best;           // ~0u: none yet
+  unsigned long long* mr_tests;
+};
+cudaError_t launch_big_filter(const BigArgs& a, uint32_t k0, uint32_t kcount, cudaStream_t s);
+cudaError_t launch_big_mr(const BigArgs& a, uint32_t k0, int grid, cudaStream_t s);
+
 // kernels/probe.cu: kind 0 = 32-bit ALU ops/s, 1 = shared-memory atomicAnd/s,
 // 2 = 64-bit Montgomery products/s
 cudaError_t run_probe(int kind, int sm_count, double* ops_per_s, cudaStream_t st);

@@ -836,6 +836,12 @@ gb_status gb_autotune_range(gb_ctx* c, uint64_t start, uint64_t limit, const gb_
   GB_PUBLIC(c, autotune_impl(c, c->ws, start, limit, base, tuned, res));
 }
 
+gb_status gb_check_big(gb_ctx* c, const uint32_t* n_limbs, uint32_t nlimbs, uint64_t p_limit,
+                       uint64_t* p_out, uint32_t* q_limbs, gb_big_result* res) {
+  if (!c) return GB_EINVAL;
+  GB_PUBLIC(c, big_impl(c, c->ws, n_limbs, nlimbs, p_limit, p_out, q_limbs, res));
+}
+
 gb_status gb_autotune_windows(gb_ctx* c, const gb_window* w, size_t count, const gb_windows_opts* base,
                               gb_windows_opts* tuned, gb_windows_tune* res) {
   if (!c) return GB_EINVAL;

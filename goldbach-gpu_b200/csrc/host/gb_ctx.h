@@ -140,6 +140,8 @@ gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint
 gb_status single_impl(gb_ctx* c, Workspace& w, Arena* arena, const uint64_t* n, size_t count,
                       uint64_t* p_out, uint64_t* q_out, const gb_single_opts* opts,
                       gb_single_result* res);
+gb_status big_impl(gb_ctx* c, Workspace& w, const uint32_t* n_limbs, uint32_t nlimbs,
+                   uint64_t p_limit, uint64_t* p_out, uint32_t* q_limbs, gb_big_result* res);
 uint64_t windows_request_bytes(const gb_window& w, const gb_windows_opts& o);
 gb_status autotune_windows_impl(gb_ctx* c, Workspace& w, const gb_window* win, size_t count,
                                 const gb_windows_opts* base, gb_windows_opts* tuned,

@@ -264,6 +264,29 @@ gb_status gb_check_single_batch_noalloc(const uint64_t* n, size_t count, uint64_
                                         uint64_t* q_out, uint64_t p_limit, void* stream);
 
 /* -------------------------------------------------------------------------
+ * Even n beyond 2^64: the minimal prime p <= p_limit with n - p a probable
+ * prime.  Replaces big_check (src/big_check.cpp:35-144), which keeps the
+ * first q accepted by GMP's 25-round mpz_probab_prime_p that its OpenMP
+ * threads find in batches of 1000 primes -- a valid partition, not
+ * guaranteed minimal.  n is given as nlimbs little-endian 32-bit limbs (n
+ * even, 4 <= n < 2^(32 GB_BIG_MAX_LIMBS)); q_limbs (nlimbs entries,
+ * nullable) receives q = n - p.  q is accepted when no prime below 4096
+ * divides it and it passes strong probable-prime tests to the 12 bases 2,
+ * 3, ..., 37 (the reference's base set, src/goldbach.cu:333-360): a proof of
+ * primality for q < 3.3e24, a probable-prime verdict beyond.  n below 2^64
+ * take gb_check_single_batch (deterministic).  *p_out = 0: no p <= p_limit
+ * (0: 1e8) gives a probable prime.
+ * ---------------------------------------------------------------------- */
+#define GB_BIG_MAX_LIMBS 128 /* n below 2^4096 (1233 decimal digits) */
+typedef struct gb_big_result {
+  uint64_t candidates;  /* candidate p examined (in whole batches)       */
+  uint64_t mr_tests;    /* strong-test runs started (trial division passed) */
+  double device_ms;
+} gb_big_result;
+gb_status gb_check_big(gb_ctx* ctx, const uint32_t* n_limbs, uint32_t nlimbs, uint64_t p_limit,
+                       uint64_t* p_out, uint32_t* q_limbs, gb_big_result* res);
+
+/* -------------------------------------------------------------------------
  * Batched windows: many independent ranges of consecutive even n.
  * ---------------------------------------------------------------------- */
 typedef struct gb_window {
