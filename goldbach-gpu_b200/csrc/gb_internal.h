@@ -162,11 +162,13 @@ cudaError_t launch_win_pairs(const WinDesc6* win, uint32_t nwin, const uint32_t*
 
 // kernels/big.cu: partitions of n beyond 2^64.  One batch of candidates
 // primes[k0 .. k0 + kcount): the filter appends the indices (from k0) whose
-// q = n - p no trial prime divides; the test lowers *best to the smallest
-// index whose q passes the 12-base strong probable-prime test.
+// q = n - p no trial prime divides; phase 0 runs the base-2 strong test on
+// them and lists the passers; phase 1 runs the 11 other bases, one thread
+// per (passer, base), and marks the passers that fail one.
 struct BigArgs {
   const uint32_t* n;        // n in `limbs` little-endian 32-bit limbs (zero-padded)
-  uint32_t limbs;           // 4, 8, 16, 32, 64 or 128
+  uint32_t limbs;           // template width: 4, 8, 16, 32, 64 or 128
+  uint32_t nl;              // n's own limbs (<= limbs): R = 2^(32 nl)
   const uint32_t* primes;
   uint64_t p_lim;           // candidates p <= p_lim
   const uint32_t* trial;    // trial primes r
@@ -174,11 +176,13 @@ struct BigArgs {
   uint32_t ntrial;
   uint32_t* surv;           // survivors (candidate index from k0)
   uint32_t* nsurv;
-  uint32_t* best;           // ~0u: none yet
+  uint32_t* pass;           // base-2 passers (candidate index from k0)
+  uint32_t* fail;           // per passer: nonzero once a base fails
+  uint32_t* npass;
   unsigned long long* mr_tests;
 };
 cudaError_t launch_big_filter(const BigArgs& a, uint32_t k0, uint32_t kcount, cudaStream_t s);
-cudaError_t launch_big_mr(const BigArgs& a, uint32_t k0, int grid, cudaStream_t s);
+cudaError_t launch_big_mr(const BigArgs& a, uint32_t k0, int phase, int grid, cudaStream_t s);
 
 // kernels/probe.cu: kind 0 = 32-bit ALU ops/s, 1 = shared-memory atomicAnd/s,
 // 2 = 64-bit Montgomery products/s

@@ -5,9 +5,10 @@
 // threads in batches of 1000 primes, keeping the first success.  Here the
 // candidates come from the resident prime table in batches of kBigBatch:
 // the filter kernel drops q = n - p with a factor below kBigTrialBound (from
-// n mod r, computed here once), the test kernel runs the 12-base strong
-// probable-prime test on the survivors (kernels/big.cu), and the smallest
-// passing candidate of the first batch that has one is the minimal p.
+// n mod r, computed here once), the base-2 kernel tests the survivors, the
+// bases kernel runs the other 11 bases on the base-2 passers in parallel
+// (kernels/big.cu), and the smallest passer no base rejects, in the first
+// batch that has one, is the minimal p.
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -68,24 +69,28 @@ gb_status big_impl(gb_ctx* c, Workspace& w, const uint32_t* n_limbs, uint32_t nl
   std::vector<uint32_t> npad(N, 0);
   std::copy(n_limbs, n_limbs + m, npad.begin());
   Temps tmp(c, nullptr);
-  void *d_n, *d_trial, *d_nmod, *d_surv, *d_small;
+  void *d_n, *d_trial, *d_nmod, *d_surv, *d_pass, *d_small;
   if ((st = ws_buffer(c, w, tmp, 0, N * 4, &d_n)) != GB_OK ||
       (st = ws_buffer(c, w, tmp, 1, trial.size() * 4, &d_trial)) != GB_OK ||
       (st = ws_buffer(c, w, tmp, 2, nmod.size() * 4, &d_nmod)) != GB_OK ||
       (st = ws_buffer(c, w, tmp, 3, kBigBatch * 4, &d_surv)) != GB_OK ||
-      (st = ws_buffer(c, w, tmp, 4, 64, &d_small)) != GB_OK)
+      (st = ws_buffer(c, w, tmp, 4, kBigBatch * 8, &d_pass)) != GB_OK ||
+      (st = ws_buffer(c, w, tmp, 5, 64, &d_small)) != GB_OK)
     return st;
   BigArgs a{};
   a.n = (const uint32_t*)d_n;
   a.limbs = N;
+  a.nl = m;
   a.primes = c->d_primes;
   a.p_lim = p_limit;
   a.trial = (const uint32_t*)d_trial;
   a.nmod = (const uint32_t*)d_nmod;
   a.ntrial = (uint32_t)trial.size();
   a.surv = (uint32_t*)d_surv;
+  a.pass = (uint32_t*)d_pass;
+  a.fail = (uint32_t*)d_pass + kBigBatch;
   a.nsurv = (uint32_t*)d_small;
-  a.best = (uint32_t*)d_small + 1;
+  a.npass = (uint32_t*)d_small + 1;
   a.mr_tests = (unsigned long long*)((char*)d_small + 8);
   cudaStream_t s = c->stream;
   cudaError_t e = cudaSuccess;
@@ -100,15 +105,24 @@ gb_status big_impl(gb_ctx* c, Workspace& w, const uint32_t* n_limbs, uint32_t nl
   uint32_t best = 0xffffffffu;
   uint64_t k0 = 1;  // p = 2 leaves q = n - 2 even
   uint32_t pk = 0;
+  std::vector<uint32_t> pass(2 * kBigBatch);
   while (k0 < np && e == cudaSuccess) {
     const uint32_t kc = (uint32_t)std::min<uint64_t>(kBigBatch, np - k0);
-    chk(cudaMemsetAsync(a.nsurv, 0, 4, s));
-    chk(cudaMemsetAsync(a.best, 0xff, 4, s));
+    chk(cudaMemsetAsync(a.nsurv, 0, 8, s));  // survivors and passers
     chk(launch_big_filter(a, (uint32_t)k0, kc, s));
-    chk(launch_big_mr(a, (uint32_t)k0, c->sm_count * 4, s));
-    chk(cudaMemcpyAsync(&best, a.best, 4, cudaMemcpyDeviceToHost, s));
+    chk(launch_big_mr(a, (uint32_t)k0, 0, c->sm_count * 4, s));
+    chk(launch_big_mr(a, (uint32_t)k0, 1, c->sm_count * 4, s));
+    uint32_t np_ = 0;
+    chk(cudaMemcpyAsync(&np_, a.npass, 4, cudaMemcpyDeviceToHost, s));
     chk(cudaStreamSynchronize(s));
     r.candidates += kc;
+    if (e == cudaSuccess && np_) {
+      chk(cudaMemcpyAsync(pass.data(), a.pass, np_ * 4, cudaMemcpyDeviceToHost, s));
+      chk(cudaMemcpyAsync(pass.data() + kBigBatch, a.fail, np_ * 4, cudaMemcpyDeviceToHost, s));
+      chk(cudaStreamSynchronize(s));
+      for (uint32_t j = 0; j < np_; ++j)
+        if (!pass[kBigBatch + j] && pass[j] < best) best = pass[j];
+    }
     if (best != 0xffffffffu) {
       chk(cudaMemcpy(&pk, c->d_primes + k0 + best, 4, cudaMemcpyDeviceToHost));
       break;
