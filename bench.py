@@ -747,6 +747,21 @@ def main():
         "result": {"checked": res0["checked"], "failures": res0["failures"],
                    "phase2_fallbacks": res0["phase2_fallbacks"], "max_minp": res0["max_minp"]},
     }
+    # C2's SEG_SIZE sweep: the segment is only the reporting unit here, so
+    # every size runs the same kernel over the same chunks (one call each)
+    sweep = []
+    if world == 1 and not args.no_extras:
+        for lg in range(24, 31):
+            segs = gb.load().gb_num_segments(start, limit, 1 << lg)
+            fb = torch.zeros(segs, dtype=torch.int32, device=dev)
+            kw2 = dict(kw, seg_size=1 << lg)
+            r = ctx.verify_range(start, limit, device_out={"minp_hist": hist, "seg_fallbacks": fb,
+                                                           "seg_failures": fb}, **kw2)
+            sweep.append({"seg_size": 1 << lg, "segments": segs, "kernel_ms": r.result["kernel_ms"],
+                          "device_ms": r.result["device_ms"],
+                          "value": total / (r.result["device_ms"] / 1e3),
+                          "failures": r.result["failures"]})
+        out["seg_size_sweep"] = sweep
     ctx.close()
     if world == 1 and rank == 0:
         if not args.no_cpu_baseline:

@@ -309,54 +309,106 @@ __device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_
     for (int i = 0; i < kWT6; ++i) live += __popc(U[i]);
   }
   const uint32_t pos0 = level6_start(L), pend = level6_end(ri, L);
-  uint32_t held = 0, kheld = 0;  // a step's count waiting for the next step's
-  bool pending = false;          // (warp-uniform)
-#pragma unroll 1
-  for (uint32_t pos = pos0; pos < pend; ++pos) {
-    if (((pos - pos0) & 7) == 0) {
-      uint32_t any = 0;
-#pragma unroll
-      for (int i = 0; i < kWT6; ++i) any |= U[i];
-      if (!__any_sync(0xffffffffu, any)) break;
-    }
-    const uint32_t e = E[pos];
-    const uint32_t q5 = e >> 31;
-    const uint32_t off = (q5 ? K5 : K1) - e6_u(e);
-    const uint32_t wo = off >> 5;
-    ca.at(q5 ? Q5 : Q1, wo, wo | (q5 << 31), W);
-    const uint32_t p = MINP ? 6 * e6_u(e) + e6_pmod(ri, q5) : 0;
-    uint32_t cnt;
-    if (MINP) {
-      cnt = step6<MINP, kWT6>(s, U, ca.lo, ca.hi, off & 31, p, W, ibase);
-    } else {
-      uint32_t now = 0;
+  if constexpr (!MINP && !LISTED) {
+    // Level 0 steps in pairs (its span starts at entry 0): the two
+    // steps' counts, at most 7 * 32 * 32 = 7168 each, share one warp
+    // reduction packed in the halves of a word, and the early-exit vote
+    // comes every fourth pair.  Each step clears the q-prime bits of the
+    // lane's words and counts the lane's unresolved n: resolved = live
+    // before - live after.
+    auto step = [&](uint32_t e) -> uint32_t {
+      const uint32_t q5 = e >> 31;
+      const uint32_t off = (q5 ? K5 : K1) - e6_u(e);
+      const uint32_t wo = off >> 5;
+      ca.at(q5 ? Q5 : Q1, wo, wo | (q5 << 31), W);
       const uint32_t sh = off & 31;
+      uint32_t now = 0;
 #pragma unroll
       for (int i = 0; i < kWT6; ++i) {
         U[i] &= ~__funnelshift_r(ca.lo[i], ca.hi[i], sh);
         now += __popc(U[i]);
       }
-      cnt = live - now;
+      const uint32_t c = live - now;
       live = now;
-    }
-    // two steps' counts (at most 7 * 32 * 32 = 7168 each) share one warp
-    // reduction, packed in the two halves of a word
-    if (pending) {
-      const uint32_t v = __reduce_add_sync(0xffffffffu, held | (cnt << 16));
-      if (lane == 0) {
-        if (v & 0xffffu) atomicAdd(&HIST[kheld], v & 0xffffu);
-        if (v >> 16) atomicAdd(&HIST[e6_k(e)], v >> 16);
+      return c;
+    };
+    uint32_t pos = pos0;
+    bool done = false;
+#pragma unroll 1
+    for (; pos + 1 < pend; pos += 2) {
+      if (((pos - pos0) & 7) == 0) {
+        uint32_t any = 0;
+#pragma unroll
+        for (int i = 0; i < kWT6; ++i) any |= U[i];
+        if (!__any_sync(0xffffffffu, any)) {
+          done = true;
+          break;
+        }
       }
-      pending = false;
-    } else {
-      held = cnt;
-      kheld = e6_k(e);
-      pending = true;
+      const uint2 ee = *reinterpret_cast<const uint2*>(E + pos);
+      const uint32_t c0 = step(ee.x);
+      const uint32_t c1 = step(ee.y);
+      const uint32_t v = __reduce_add_sync(0xffffffffu, c0 | (c1 << 16));
+      if (lane == 0) {
+        if (v & 0xffffu) atomicAdd(&HIST[e6_k(ee.x)], v & 0xffffu);
+        if (v >> 16) atomicAdd(&HIST[e6_k(ee.y)], v >> 16);
+      }
     }
-  }
-  if (pending) {
-    const uint32_t v = __reduce_add_sync(0xffffffffu, held);
-    if (lane == 0 && v) atomicAdd(&HIST[kheld], v);
+    if (!done && pos < pend) {  // an odd last entry
+      const uint32_t e = E[pos];
+      const uint32_t v = __reduce_add_sync(0xffffffffu, step(e));
+      if (lane == 0 && v) atomicAdd(&HIST[e6_k(e)], v);
+    }
+  } else {
+    uint32_t held = 0, kheld = 0;  // a step's count waiting for the next step's
+    bool pending = false;          // (warp-uniform)
+#pragma unroll 1
+    for (uint32_t pos = pos0; pos < pend; ++pos) {
+      if (((pos - pos0) & 7) == 0) {
+        uint32_t any = 0;
+#pragma unroll
+        for (int i = 0; i < kWT6; ++i) any |= U[i];
+        if (!__any_sync(0xffffffffu, any)) break;
+      }
+      const uint32_t e = E[pos];
+      const uint32_t q5 = e >> 31;
+      const uint32_t off = (q5 ? K5 : K1) - e6_u(e);
+      const uint32_t wo = off >> 5;
+      ca.at(q5 ? Q5 : Q1, wo, wo | (q5 << 31), W);
+      uint32_t cnt;
+      if (MINP) {
+        const uint32_t p = 6 * e6_u(e) + e6_pmod(ri, q5);
+        cnt = step6<MINP, kWT6>(s, U, ca.lo, ca.hi, off & 31, p, W, ibase);
+      } else {  // clear and count the lane's unresolved n (live before - after)
+        uint32_t now = 0;
+        const uint32_t sh = off & 31;
+#pragma unroll
+        for (int i = 0; i < kWT6; ++i) {
+          U[i] &= ~__funnelshift_r(ca.lo[i], ca.hi[i], sh);
+          now += __popc(U[i]);
+        }
+        cnt = live - now;
+        live = now;
+      }
+      // two steps' counts (at most 7 * 32 * 32 = 7168 each) share one warp
+      // reduction, packed in the two halves of a word
+      if (pending) {
+        const uint32_t v = __reduce_add_sync(0xffffffffu, held | (cnt << 16));
+        if (lane == 0) {
+          if (v & 0xffffu) atomicAdd(&HIST[kheld], v & 0xffffu);
+          if (v >> 16) atomicAdd(&HIST[e6_k(e)], v >> 16);
+        }
+        pending = false;
+      } else {
+        held = cnt;
+        kheld = e6_k(e);
+        pending = true;
+      }
+    }
+    if (pending) {
+      const uint32_t v = __reduce_add_sync(0xffffffffu, held);
+      if (lane == 0 && v) atomicAdd(&HIST[kheld], v);
+    }
   }
   if (L + 1 < kLevels6) {
     uint2* out = surv6_list(L & 1, ri);
