@@ -423,6 +423,50 @@ def measure_counts(gb, ctx, points=((10**9, 4096), (10**10, 1024))):
     return out
 
 
+def measure_c1(gb, ctx, device):
+    """C1 as stated: every even n in [4, 1e9], SEG_SIZE 2^26, P_SMALL 1e8, the
+    per-n outputs (minimal p as uint32, 2 GB; the verified bitmap) -- on the
+    device (kernel + device time), and end to end through the C-ABI into
+    pinned host buffers (the 2 GB device-to-host copy inside the timing)."""
+    import numpy as np
+    import torch
+    lim, seg = 10**9, 1 << 26
+    count = (lim - 4) // 2 + 1
+    words = (count + 31) // 32
+    dev = torch.device("cuda", device)
+    d_minp = torch.empty(count, dtype=torch.int32, device=dev)
+    d_bits = torch.empty(words, dtype=torch.int32, device=dev)
+    d_hist = torch.zeros(4096, dtype=torch.int64, device=dev)
+    kw = dict(seg_size=seg, p_small=10**8)
+    ctx.verify_range(4, lim, device_out={"min_p": d_minp, "verified_bits": d_bits,
+                                         "minp_hist": d_hist}, **kw)  # warm
+    r = ctx.verify_range(4, lim, device_out={"min_p": d_minp, "verified_bits": d_bits,
+                                             "minp_hist": d_hist}, **kw).result
+    del d_minp, d_bits
+    h_minp = torch.empty(count, dtype=torch.int32).pin_memory()
+    h_bits = torch.empty(words, dtype=torch.int32).pin_memory()
+    h_hist = torch.empty(4096, dtype=torch.int64).pin_memory()
+    L = gb.load()
+    o = gb.RangeOpts(seg, 10**8, 0, 0, 0, 0, 1, 0, None, 0)
+    out = gb.RangeOut(h_bits.data_ptr(), h_minp.data_ptr(), h_hist.data_ptr(), None, None, None)
+    res = gb.RangeResult()
+    walls = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        st = L.gb_verify_range(ctx._h, 4, lim, ctypes.byref(o), ctypes.byref(res), ctypes.byref(out))
+        walls.append(time.perf_counter() - t0)
+        if st != 0:
+            raise RuntimeError(f"gb_verify_range failed: {st}")
+    e2e = min(walls)
+    mp = h_minp.numpy()
+    return {"workload": "[4, 1e9], seg 2^26, P_SMALL 1e8, per-n minimal p + verified bitmap",
+            "even_n": count, "kernel_ms": r["kernel_ms"], "device_ms": r["device_ms"],
+            "value": count / (r["device_ms"] / 1e3), "e2e_value": count / e2e, "e2e_ms": e2e * 1e3,
+            "d2h_bytes_per_step": count * 4 + words * 4 + 4096 * 8, "unit": UNIT,
+            "failures": res.failures, "max_minp": int(mp.max()),
+            "min_p_sha256": __import__("hashlib").sha256(mp.tobytes()).hexdigest()}
+
+
 # the reference's published flags for its GPU verifier (RESULTS.md:39-41)
 REF_GPU_FLAGS = ["--seg-size=200000000", "--p-small=1000000", "--batch-size=2000000"]
 
@@ -548,7 +592,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--ref-sample-log2", type=int, default=24)
-    ap.add_argument("--extra", choices=["windows", "single", "counts", "serving", "reference_gpu"],
+    ap.add_argument("--extra", choices=["windows", "single", "counts", "serving", "reference_gpu", "c1"],
                     help="run only this secondary measurement and print its JSON (profiling)")
     ap.add_argument("--windows", type=int, default=4096,
                     help="--extra windows: the first N seeded windows only")
@@ -570,6 +614,8 @@ def main():
                                                      not args.no_windows_tune)))
                 elif args.extra == "reference_gpu":
                     print(json.dumps(measure_reference_gpu(gb, c, 0)))
+                elif args.extra == "c1":
+                    print(json.dumps(measure_c1(gb, c, 0)))
                 else:
                     f = {"single": measure_single, "counts": measure_counts}
                     print(json.dumps(f[args.extra](gb, c)))
@@ -769,6 +815,7 @@ def main():
         if not args.no_extras:
             with gb.Context(local) as c2:
                 out["reference_gpu"] = measure_reference_gpu(gb, c2, local)
+                out["c1"] = measure_c1(gb, c2, local)
                 out["windows"] = measure_windows(gb, c2)
                 out["single"] = measure_single(gb, c2)
                 out["counts"] = measure_counts(gb, c2)

@@ -145,6 +145,8 @@ void ws_free(gb_ctx* c, Workspace& w) {
   w.queue = nullptr;
   w.scratch = nullptr;
   w.scratch_bytes = 0;
+  if (w.win_exec) cudaGraphExecDestroy(w.win_exec);
+  w.win_exec = nullptr;
   for (cudaEvent_t* e : {&w.ev0, &w.ev1, &w.ek0, &w.ek1, &w.ek2})
     if (*e) {
       cudaEventDestroy(*e);

@@ -45,6 +45,7 @@ struct Workspace {
   QEntry* queue = nullptr;
   uint32_t queue_cap = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ek0 = nullptr, ek1 = nullptr, ek2 = nullptr;
+  cudaGraphExec_t win_exec = nullptr;  // the windows batch's launches (updated per batch)
   void* scratch = nullptr;  // per-call kernel scratch, grown on demand
   size_t scratch_bytes = 0;
   // per-call device buffers of the public entry points (slot i grown on

@@ -4,9 +4,10 @@
 // offsets in [1e15, 1e18]) in one batch.  The reference has no batch mode:
 // each window would be one `goldbach --start=A LIMIT` process with its own
 // segment loop (src/goldbach.cu:420-485).  GB_WINDOWS_PERSISTENT runs the
-// batch as three launches: the large-prime pass over every window's class
-// masks (kernels/windows.cu), range6_kernel in windows mode over every
-// (window, chunk) item from one device work counter, and the device Phase 2.
+// batch as one CUDA graph of three launches: the large-prime pass over
+// every window's class masks (kernels/windows.cu), range6_kernel in windows
+// mode over every (window, chunk) item from one device work counter, and the
+// device Phase 2.
 // GB_WINDOWS_PLAIN runs the same launches window by window (the per-window
 // launch pipeline, kept for comparison).
 #include <algorithm>
@@ -219,18 +220,46 @@ static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, cons
   float large_ms = 0, search_ms = 0;
   chk(cudaEventRecord(ws.ev0, s));
   if (o.mode == GB_WINDOWS_PERSISTENT) {
+    // The batch's launches as one CUDA graph: captured per call (the
+    // arguments change), applied to the workspace's executable graph by an
+    // in-place update -- the topology repeats from batch to batch, so the
+    // graph is instantiated once and relaunched -- and launched as one unit.
+    // A caller that is itself capturing the stream gets the launches inline.
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    chk(cudaStreamIsCapturing(s, &cs));
+    const bool graph = e == cudaSuccess && cs == cudaStreamCaptureStatusNone;
+    auto mark = [&](cudaEvent_t ev) {  // timing events: nodes of the graph
+      chk(graph ? cudaEventRecordWithFlags(ev, s, cudaEventRecordExternal) : cudaEventRecord(ev, s));
+    };
+    if (graph) chk(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     chk(cudaMemsetAsync(d_lmask, 0xff, lwords_total * 4, s));
-    chk(cudaEventRecord(ws.ek0, s));
+    mark(ws.ek0);
     if (la.k1 > la.k0) {
       chk(launch_win_large(la, gl, s));
       ++launches;
     }
-    chk(cudaEventRecord(ws.ek1, s));
+    mark(ws.ek1);
     const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(grid_max, a.total_items));
     chk(launch_range(a, grid, s));
-    chk(cudaEventRecord(ws.ek2, s));
+    mark(ws.ek2);
     chk(launch_fallback(sp, sm * 4, s));
     launches += 2;
+    if (graph) {
+      cudaGraph_t g = nullptr;
+      const cudaError_t ec = cudaStreamEndCapture(s, &g);  // ends the capture in every case
+      chk(ec);
+      if (e == cudaSuccess) {
+        cudaGraphExecUpdateResultInfo info{};
+        if (!ws.win_exec || cudaGraphExecUpdate(ws.win_exec, g, &info) != cudaSuccess) {
+          cudaGetLastError();  // another topology: instantiate anew
+          if (ws.win_exec) cudaGraphExecDestroy(ws.win_exec);
+          ws.win_exec = nullptr;
+          chk(cudaGraphInstantiate(&ws.win_exec, g, 0));
+        }
+        if (e == cudaSuccess) chk(cudaGraphLaunch(ws.win_exec, s));
+      }
+      if (g) cudaGraphDestroy(g);
+    }
   } else {
     for (uint32_t r = 0; r < count && e == cudaSuccess; ++r) {
       const WinDesc6& d = desc[r];
