@@ -53,7 +53,9 @@ __device__ __forceinline__ uint32_t find_item_window(const uint64_t* off, uint32
   return lo;
 }
 
-template <bool MINP, int NT>
+// WIN: windows mode (a.win set) -- a template parameter so that the range
+// instantiation carries none of its state through the inlined sieve.
+template <bool MINP, int NT, bool WIN>
 __global__ void __launch_bounds__(NT, 1024 / NT) range6_kernel(const __grid_constant__ RangeArgs a) {
   const SearchParams& s = a.s;
   __shared__ unsigned long long s_item;
@@ -79,7 +81,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) range6_kernel(const __grid_cons
   for (;;) {
     if (tid == 0) {
       s_item = atomicAdd(&s.ctr[kCtrWork], 1ull);
-      if (a.win && s_item < a.total_items) {
+      if (WIN && s_item < a.total_items) {
         const uint32_t w = find_item_window(a.chunk_off, a.nwin, s_item);
         const WinDesc6 d = a.win[w];
         const uint64_t j0 = (s_item - a.chunk_off[w]) * a.chunk_evens;
@@ -106,7 +108,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) range6_kernel(const __grid_cons
     if (item >= a.total_items) break;
     uint64_t A, base_idx, unit;
     uint32_t cnt;
-    if (a.win) {
+    if (WIN) {
       A = s_wA;
       cnt = s_wcnt;
       base_idx = s_wbase;
@@ -154,7 +156,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) range6_kernel(const __grid_cons
     const uint32_t* L1 = nullptr;
     const uint32_t* L5 = nullptr;
     uint32_t lsh = 0;
-    if (a.win) {  // the window's large-prime mask from this chunk's base on
+    if (WIN) {  // the window's large-prime mask from this chunk's base on
       const uint64_t d = (uint64_t)(G0 - s_wg0);
       L1 = a.lmask + s_wlbase + (d >> 5);
       L5 = L1 + s_wlwords;
@@ -255,13 +257,22 @@ static int occupancy(K kernel, size_t smem, int threads) {
 template <typename F>
 static cudaError_t with_range_kernel(const RangeArgs& a, F f) {
   const uint32_t nt = a.threads ? a.threads : kRange6DefaultThreads;
-  const bool mp = a.s.minp != nullptr;
+  const int v = (a.s.minp != nullptr ? 1 : 0) + (a.win != nullptr ? 2 : 0);
+#define GB_RANGE_SHAPE(T)                                 \
+  case T:                                                 \
+    switch (v) {                                          \
+      case 0: return f(range6_kernel<false, T, false>, T); \
+      case 1: return f(range6_kernel<true, T, false>, T);  \
+      case 2: return f(range6_kernel<false, T, true>, T);  \
+      default: return f(range6_kernel<true, T, true>, T);  \
+    }
   switch (nt) {
-    case 256: return mp ? f(range6_kernel<true, 256>, 256) : f(range6_kernel<false, 256>, 256);
-    case 512: return mp ? f(range6_kernel<true, 512>, 512) : f(range6_kernel<false, 512>, 512);
-    case 1024: return mp ? f(range6_kernel<true, 1024>, 1024) : f(range6_kernel<false, 1024>, 1024);
+    GB_RANGE_SHAPE(256)
+    GB_RANGE_SHAPE(512)
+    GB_RANGE_SHAPE(1024)
     default: return cudaErrorInvalidValue;
   }
+#undef GB_RANGE_SHAPE
 }
 
 int range_max_blocks_per_sm(const RangeArgs& a) {
