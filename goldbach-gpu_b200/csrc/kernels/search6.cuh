@@ -217,7 +217,7 @@ struct Cache6 {
 };
 
 // One lockstep step: the U words of a lane against one prime p.  No mask
-// for p > n/2 is needed (unlike the odd-only search): a partition n = p + q
+// for p > n/2 is needed: a partition n = p + q
 // with q < p would have been found at the smaller prime q, which is in the
 // same class sequence, and every q < 5 reads a cleared bit.
 template <bool MINP, int WT, typename Words>

@@ -415,7 +415,8 @@ typedef struct gb_serve_opts {
   uint64_t max_n;              /* largest n served (0: 2^64 - 1)               */
   uint32_t max_single_batch;   /* n per single-lane batch (0: 2^18)            */
   uint32_t max_range_batch;    /* requests per range-lane batch (0: 4096)      */
-  uint64_t range_arena_bytes;  /* range-lane device memory (0: 4 GiB)          */
+  uint64_t range_arena_bytes;  /* the range lanes' pool when pool_bytes is 0
+                                  (0: see pool_bytes)                        */
   uint64_t small_range;        /* ranges of <= this many n run n by n (0: 2^15) */
   uint32_t no_graph;           /* 1: single-lane batches of < 8192 n as plain
                                   stream launches instead of one CUDA graph   */
