@@ -514,7 +514,8 @@ def measure_reference_gpu(gb, ctx, device, limits=(10**9, 10**10, 10**11)):
 SERVE_SPIN_US = 20000
 
 
-def measure_serving(gb, device, rates=(1e2, 1e3, 1e4, 1e5), seconds=2.0, max_requests=10000):
+def measure_serving(gb, device, rates=(1e2, 1e3, 1e4, 1e5), seconds=2.0, max_requests=10000,
+                    range_lanes=0, max_range_batch=0):
     """C5: Poisson arrivals (seed 3) per rate; 70% single n uniform in
     [4, 2^64-2], 30% ranges of log-uniform width 2^8..2^26 even n at
     offsets uniform in [4, 1e19]; latency from scheduled arrival.  The
@@ -523,7 +524,8 @@ def measure_serving(gb, device, rates=(1e2, 1e3, 1e4, 1e5), seconds=2.0, max_req
     import numpy as np
     out = []
     with gb.Context(device) as ctx:
-        ctx.serve_start(max_n=2**64 - 1, spin_us=SERVE_SPIN_US)
+        ctx.serve_start(max_n=2**64 - 1, spin_us=SERVE_SPIN_US, range_lanes=range_lanes,
+                        max_range_batch=max_range_batch)
         for rate in rates:
             rng = np.random.default_rng(3)
             m = int(min(max_requests, rate * seconds))
@@ -559,7 +561,8 @@ def measure_serving(gb, device, rates=(1e2, 1e3, 1e4, 1e5), seconds=2.0, max_req
             out.append({"rate_rps": rate, "lane_spin_us": SERVE_SPIN_US, "requests": m,
                         "completed": sum(r["status"] == 0 for r in res),
                         "rejected": st["rejected"], "busy": st["busy"],
-                        "range_lanes": 2, "pool_bytes": st["pool_bytes"],
+                        "range_lanes": range_lanes or 2, "max_range_batch": max_range_batch or 4096,
+                        "pool_bytes": st["pool_bytes"],
                         "pool_peak_bytes": st["pool_peak_bytes"],
                         "p50_us": st["p50_us"], "p99_us": st["p99_us"],
                         "single_p50_us": float(np.percentile(lat_s, 50)) if lat_s.size else None,
@@ -598,6 +601,11 @@ def main():
                     help="--extra windows: the first N seeded windows only")
     ap.add_argument("--no-windows-plain", action="store_true",
                     help="--extra windows: skip the plain per-window pipeline")
+    ap.add_argument("--serve-rates", default="100,1000,10000,100000",
+                    help="--extra serving: request rates (comma-separated)")
+    ap.add_argument("--serve-lanes", type=int, default=0, help="--extra serving: range lanes (0: default)")
+    ap.add_argument("--serve-range-batch", type=int, default=0,
+                    help="--extra serving: requests per range-lane batch (0: default)")
     ap.add_argument("--no-windows-tune", action="store_true",
                     help="--extra windows: default knobs instead of the windows autotuner's")
     args = ap.parse_args()
@@ -606,7 +614,9 @@ def main():
     if args.extra:
         gb = load_gb()
         if args.extra == "serving":
-            print(json.dumps(measure_serving(gb, 0)))
+            rates = tuple(float(x) for x in args.serve_rates.split(","))
+            print(json.dumps(measure_serving(gb, 0, rates, range_lanes=args.serve_lanes,
+                                             max_range_batch=args.serve_range_batch)))
         else:
             with gb.Context(0) as c:
                 if args.extra == "windows":
