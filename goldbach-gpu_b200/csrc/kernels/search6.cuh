@@ -36,7 +36,7 @@ namespace gb {
 constexpr int kSmemHistBins = 1024;  // per-CTA minimal-p histogram bins in shared memory
 
 constexpr uint32_t kE6UBits = 15;
-constexpr uint32_t kLockSteps6 = 128; // lockstep entries of each class sequence
+constexpr uint32_t kLockSteps6 = 256; // lockstep entries of each class sequence (prime index < 1024: the shared histogram)
 // The lockstep runs in levels: level 0 takes every word of the chunk through
 // the entries [0, 28); each later level takes the words still holding an
 // unresolved n (a per-class survivor list written by the level before it,

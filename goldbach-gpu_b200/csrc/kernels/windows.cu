@@ -95,7 +95,15 @@ __device__ __forceinline__ LargePrime large_prime(const WinLargeArgs& a, uint32_
   const uint2 ac = __ldg(a.a15 + k);
   q.a1 = ac.x;
   q.dl = ac.y >= ac.x ? ac.y - ac.x : ac.y + q.p - ac.x;
-  q.inv = 1.0 / (double)q.p;
+  // 1/p to a relative error near 2^-47: the single-precision reciprocal
+  // (2^-23 with the rounding of p to a float) and one Newton step in double
+  // precision.  The quotient estimate needs |g0/p| * error < 1/4 with
+  // g0/p < 2^42, i.e. 2^-44; a correctly rounded division costs several
+  // times more and is paid once per prime, which dominates when few
+  // windows share the pass.
+  const double pd = (double)q.p;
+  const double r0 = (double)__frcp_rn((float)q.p);
+  q.inv = fma(r0, fma(-pd, r0, 1.0), r0);
   return q;
 }
 
