@@ -89,12 +89,30 @@ struct LargePrime {
   double inv;
 };
 
+// The class offsets: from the a15 table when many windows share the pass
+// (its cost is per pair), or from p alone when few do (the pass is then paid
+// per prime, and the table's 8 bytes per prime are two thirds of what it
+// streams): 6 divides p - 1 or p + 1, so -1/6 = (p - 1)/6 for p = 1 (mod 6)
+// and p - (p + 1)/6 for p = 5 (mod 6), and a5 - a1 = 4 a1 (mod p).
+// Measured: 1.227 -> 1.073 ms for one 2^26-n window near 1e19, but
+// 119.3 -> 121.7 ms for the 4096 seeded windows without the table.
+constexpr uint32_t kLargeTableWindows = 64;
+
 __device__ __forceinline__ LargePrime large_prime(const WinLargeArgs& a, uint32_t k) {
   LargePrime q;
   q.p = __ldg(a.primes + k);
-  const uint2 ac = __ldg(a.a15 + k);
-  q.a1 = ac.x;
-  q.dl = ac.y >= ac.x ? ac.y - ac.x : ac.y + q.p - ac.x;
+  if (a.w_hi - a.w_lo >= kLargeTableWindows) {
+    const uint2 ac = __ldg(a.a15 + k);
+    q.a1 = ac.x;
+    q.dl = ac.y >= ac.x ? ac.y - ac.x : ac.y + q.p - ac.x;
+  } else {
+    const uint32_t q6 = __umulhi(q.p, 0xAAAAAAABu) >> 2;  // floor(p / 6)
+    q.a1 = q.p - 6 * q6 == 1 ? q6 : q.p - q6 - 1;
+    uint32_t d = q.a1 + q.a1;  // 4 a1 mod p in two doublings (p < 2^31)
+    d = min(d, d - q.p);
+    d = d + d;
+    q.dl = min(d, d - q.p);
+  }
   // 1/p to a relative error near 2^-47: the single-precision reciprocal
   // (2^-23 with the rounding of p to a float) and one Newton step in double
   // precision.  The quotient estimate needs |g0/p| * error < 1/4 with
