@@ -78,6 +78,11 @@ struct __align__(16) WinLarge {
   uint32_t lbits;
 };
 
+// With per-n output (SearchParams::minp) the chunks hold at most this many
+// even n: a byte per n in shared memory keeps the entry position that
+// resolved it until the chunk writes its minimal p out in n order.
+constexpr uint32_t kMinpChunk = 1u << 16;
+
 struct RangeArgs {
   SearchParams s;
   uint64_t start;          // first even n of the range

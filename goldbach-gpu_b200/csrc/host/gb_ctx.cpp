@@ -327,6 +327,7 @@ gb_status range_impl(gb_ctx* c, Workspace& w, Arena* arena, uint64_t start, uint
   }
   if (NE < 8192 || NE > (1u << 20) || (NE & (NE - 1)))
     return fail(w, GB_EINVAL, "chunk_evens must be a power of two in [2^13, 2^20]");
+  if (out && out->min_p && NE > kMinpChunk) NE = kMinpChunk;  // per-n output: smaller chunks
   if (o.block_threads && o.block_threads != 256 && o.block_threads != 512 && o.block_threads != 1024)
     return fail(w, GB_EINVAL, "block_threads must be 256, 512 or 1024");
   const uint32_t sc = o.shard_count ? o.shard_count : 1;

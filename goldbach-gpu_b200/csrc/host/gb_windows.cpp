@@ -50,9 +50,10 @@ static gb_status windows_sieve_impl(gb_ctx* c, Workspace& ws, Arena* arena, cons
   if (count > 0xffffffffull) return fail(ws, GB_EINVAL, "too many windows");
   const uint32_t H = o.halo ? o.halo : 32768u;
   if (H < 128 || H > (1u << 17) || (H & 63)) return fail(ws, GB_EINVAL, "halo must be a multiple of 64 in [128, 2^17]");
-  const uint32_t NE = o.chunk_evens ? o.chunk_evens : (1u << 20);
+  uint32_t NE = o.chunk_evens ? o.chunk_evens : (1u << 20);
   if (NE < 8192 || NE > (1u << 20) || (NE & (NE - 1)))
     return fail(ws, GB_EINVAL, "chunk_evens must be a power of two in [2^13, 2^20]");
+  if (min_p_concat && NE > kMinpChunk) NE = kMinpChunk;  // per-n output: smaller chunks
   if (o.block_threads && o.block_threads != 256 && o.block_threads != 512 && o.block_threads != 1024)
     return fail(ws, GB_EINVAL, "block_threads must be 256, 512 or 1024");
   const uint64_t p_lim = o.phase2_limit ? o.phase2_limit : GB_PHASE2_LIMIT_DEFAULT;

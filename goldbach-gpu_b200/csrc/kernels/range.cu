@@ -103,6 +103,10 @@ __global__ void __launch_bounds__(NT, 1024 / NT) range6_kernel(const __grid_cons
       cx.maxk = 0;
     }
     for (uint32_t i = tid; i < kSmemHistBins; i += NT) HIST[i] = 0;
+    if (MINP) {  // no n resolved yet
+      uint32_t* X = reinterpret_cast<uint32_t*>(smem6_eidx());
+      for (uint32_t i = tid; i < a.chunk_evens / 4; i += NT) X[i] = 0xffffffffu;
+    }
     __syncthreads();
     const unsigned long long item = s_item;
     if (item >= a.total_items) break;
@@ -135,6 +139,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) range6_kernel(const __grid_cons
       cx.A = A;
       cx.base_idx = base_idx;
       cx.unit = unit;
+      cx.cnt = cnt;
       const uint64_t last = A + 2ull * (cnt - 1);
       const uint32_t amod = (uint32_t)(A % 6);
       // A - 6 G0 is in [H + 1, H + 7), so every X fits 32 bits
@@ -241,7 +246,7 @@ uint32_t range6_words(uint32_t halo, uint32_t chunk_evens) {
 }
 
 size_t range_smem_bytes(const RangeArgs& a) {
-  return range6_smem_words(a.nbw) * sizeof(uint32_t);
+  return range6_smem_words(a.nbw, a.s.minp ? a.chunk_evens : 0) * sizeof(uint32_t);
 }
 
 template <typename K>

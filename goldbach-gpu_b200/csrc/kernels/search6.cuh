@@ -36,7 +36,12 @@ namespace gb {
 constexpr int kSmemHistBins = 1024;  // per-CTA minimal-p histogram bins in shared memory
 
 constexpr uint32_t kE6UBits = 15;
-constexpr uint32_t kLockSteps6 = 256; // lockstep entries of each class sequence (prime index < 1024: the shared histogram)
+constexpr uint32_t kLockSteps6 = 256;  // table stride of each class sequence
+// entries used: at most 255, so that an entry position fits a byte below the
+// per-n output's "not from the lockstep" marker 0xFF (and the prime index
+// stays below 1024, the shared histogram)
+constexpr uint32_t kLockEntries6 = kLockSteps6 - 1;
+
 // The lockstep runs in levels: level 0 takes every word of the chunk through
 // the entries [0, 28); each later level takes the words still holding an
 // unresolved n (a per-class survivor list written by the level before it,
@@ -67,6 +72,7 @@ struct Ctx6 {
   uint64_t A;         // first even n
   uint64_t base_idx;  // output index of n = A
   uint64_t unit;      // segment (range) or caller's window index (windows)
+  uint32_t cnt;       // even n in the chunk
   uint64_t n[3];      // n_rho: first n of each class
   uint32_t M[3];      // n of each class
   uint32_t K[3][2];   // K for q-class 1 and 5
@@ -105,8 +111,13 @@ __device__ __forceinline__ uint32_t* smem6_hist() { return g_smem6 + kWheel6Word
 __device__ __forceinline__ uint32_t* smem6_etab(int ri) {
   return smem6_hist() + kSmemHistBins + ri * kLockSteps6;
 }
-__host__ __device__ constexpr size_t range6_smem_words(uint32_t nbw) {
-  return kWheel6Words + 2 * (size_t)nbw + kSmemHistBins + 3 * kLockSteps6;
+// per-n output: the entry position of each n of the chunk resolved in the
+// lockstep (0xFF: resolved elsewhere, its minimal p written directly)
+__device__ __forceinline__ uint8_t* smem6_eidx() {
+  return reinterpret_cast<uint8_t*>(smem6_etab(0) + 3 * kLockSteps6);
+}
+__host__ __device__ constexpr size_t range6_smem_words(uint32_t nbw, uint32_t eidx_bytes = 0) {
+  return kWheel6Words + 2 * (size_t)nbw + kSmemHistBins + 3 * kLockSteps6 + (eidx_bytes + 3) / 4;
 }
 
 __device__ __forceinline__ uint32_t e6_u(uint32_t e) { return e & ((1u << kE6UBits) - 1); }
@@ -220,12 +231,16 @@ struct Cache6 {
 // for p > n/2 is needed: a partition n = p + q
 // with q < p would have been found at the smaller prime q, which is in the
 // same class sequence, and every q < 5 reads a cleared bit.
+// With per-n output (MINP) the entry position pos of every n the step
+// resolves goes to the chunk's byte array at the n's index in the chunk
+// (jbase + 3 m for bit m of the class); the chunk writes the minimal p out
+// in n order at its end (search_chunk6).
 template <bool MINP, int WT, typename Words>
-__device__ __forceinline__ uint32_t step6(const SearchParams& s, uint32_t (&U)[WT],
-                                          const uint32_t (&lo)[WT], const uint32_t (&hi)[WT],
-                                          uint32_t sh, uint32_t p, const Words& W,
-                                          uint64_t ibase) {  // p: MINP only
+__device__ __forceinline__ uint32_t step6(uint32_t (&U)[WT], const uint32_t (&lo)[WT],
+                                          const uint32_t (&hi)[WT], uint32_t sh, uint32_t pos,
+                                          const Words& W, uint32_t jbase) {  // pos, jbase: MINP only
   uint32_t cnt = 0;
+  uint8_t* X = smem6_eidx();
 #pragma unroll
   for (int i = 0; i < WT; ++i) {
     uint32_t h = U[i] & __funnelshift_r(lo[i], hi[i], sh);
@@ -233,11 +248,11 @@ __device__ __forceinline__ uint32_t step6(const SearchParams& s, uint32_t (&U)[W
     cnt += __popc(h);
     if (MINP) {
       if (h) {
-        const uint64_t m0 = 32ull * W[i];
+        const uint32_t m0 = 32 * W[i];
         while (h) {
           const int b = __ffs(h) - 1;
           h &= h - 1;
-          s.minp[ibase + 3 * (m0 + b)] = p;
+          X[jbase + 3 * (m0 + b)] = (uint8_t)pos;
         }
       }
     }
@@ -299,7 +314,7 @@ __device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_
   const uint32_t* __restrict__ Q5 = smem6_q(1);
   uint32_t* HIST = smem6_hist();
   const uint32_t K1 = cx.K[ri][0], K5 = cx.K[ri][1];
-  const uint64_t ibase = cx.base_idx + ((n0 - cx.A) >> 1);
+  const uint32_t jbase = (uint32_t)((n0 - cx.A) >> 1);  // index of n0 in the chunk
   Cache6<kWT6> ca;
   // without per-n output the step clears bits with one operation per word
   // and counts the lane's unresolved n: resolved = live before - live after
@@ -377,8 +392,7 @@ __device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_
       ca.at(q5 ? Q5 : Q1, wo, wo | (q5 << 31), W);
       uint32_t cnt;
       if (MINP) {
-        const uint32_t p = 6 * e6_u(e) + e6_pmod(ri, q5);
-        cnt = step6<MINP, kWT6>(s, U, ca.lo, ca.hi, off & 31, p, W, ibase);
+        cnt = step6<MINP, kWT6>(U, ca.lo, ca.hi, off & 31, pos, W, jbase);
       } else {  // clear and count the lane's unresolved n (live before - after)
         uint32_t now = 0;
         const uint32_t sh = off & 31;
@@ -487,6 +501,20 @@ __device__ __forceinline__ void search_chunk6(const SearchParams& s) {
   // the chunk's figures: the tails' (in g_cx6) plus fallbacks, largest and
   // summed minimal p read off the histogram
   __syncthreads();
+  if (MINP) {  // the lockstep's minimal p of every n, written out in n order
+    const uint8_t* X = smem6_eidx();
+    const uint32_t cnt = g_cx6.cnt;
+    const uint32_t amod = (uint32_t)(g_cx6.A % 6);
+    uint32_t* out = s.minp + g_cx6.base_idx;
+    for (uint32_t j = tid; j < cnt; j += NT) {
+      const uint32_t e = X[j];
+      if (e != 0xFFu) {
+        const int ri = (int)(((amod + 2 * (j % 3)) % 6) >> 1);  // (A + 2j) mod 6 = 2 ri
+        const uint32_t en = smem6_etab(ri)[e];
+        out[j] = 6 * e6_u(en) + e6_pmod(ri, en >> 31);
+      }
+    }
+  }
   const uint32_t* HIST = smem6_hist();
   const uint64_t unit = g_cx6.unit;
   uint32_t fbh = 0, maxk = 0;
@@ -537,7 +565,7 @@ __device__ __forceinline__ void load_tables6(const SearchParams& s) {
     uint32_t* E4 = smem6_etab(2);
     const int lane = threadIdx.x;
     const uint32_t ns = s.nsearch;
-    constexpr uint32_t L = kLockSteps6;
+    constexpr uint32_t L = kLockEntries6;
     uint32_t n0 = 0, n2 = 1, n4 = 1, k0end = 2, k2end = 2, k4end = 2;
     for (uint32_t kb = 2; kb < ns && (n0 < L || n2 < L || n4 < L); kb += 32) {
       const uint32_t k = kb + lane;
