@@ -433,13 +433,7 @@ gb_status windows_impl(gb_ctx* c, Workspace& ws, Arena* arena, const gb_window* 
     uint64_t lim = o.mr_below;
     if (!lim) {
       const double r = std::sqrt((double)last);
-      // the sieve path's large-prime pass costs about 1 ps per (prime,
-      // window) pair plus 7 ps per prime once per batch, the Miller-Rabin
-      // path about 3 ns per n: a small batch shares the per-prime part among
-      // few windows, so its split moves up (divisor 2600 for thousands of
-      // windows, about 325 for one)
-      const double div = o.mr_divisor ? (double)o.mr_divisor
-                                      : kMrBelowDivisor * (double)count / ((double)count + 7.0);
+      const double div = o.mr_divisor ? (double)o.mr_divisor : kMrBelowDivisor;
       lim = r > 1e4 ? (uint64_t)(1.1 * r / std::log(r) / div) : 0;
     }
     narrow[i] = w[i].count < lim;
@@ -506,8 +500,7 @@ uint64_t windows_request_bytes(const gb_window& w, const gb_windows_opts& o) {
   uint64_t lim = o.mr_below;
   if (!lim) {
     const double r = std::sqrt((double)last);
-    // the split of a one-window batch: the widest the Miller-Rabin path gets
-    const double div = o.mr_divisor ? (double)o.mr_divisor : kMrBelowDivisor / 8.0;
+    const double div = o.mr_divisor ? (double)o.mr_divisor : kMrBelowDivisor;
     lim = r > 1e4 ? (uint64_t)(1.1 * r / std::log(r) / div) : 0;
   }
   const uint64_t fixed = sizeof(WinDesc6) + sizeof(WinLarge) + 24 + 4 + 16 + 16 + 4 * 256;

@@ -310,8 +310,7 @@ typedef struct gb_windows_opts {
                              kernel).  0: automatic, where sieving would
                              cost more (about pi(sqrt(top)) / mr_divisor
                              n); 1: never                                  */
-  uint32_t mr_divisor;    /* the automatic split's divisor (0: 2600 B/(B+7)
-                             for a batch of B windows)                     */
+  uint32_t mr_divisor;    /* the automatic split's divisor (0: 2600)        */
   uint32_t large_ctas_per_sm; /* grid of the large-prime pass (0: 64)       */
   uint32_t block_threads; /* as gb_range_opts.block_threads (0: 512)        */
   uint32_t gpu_share_pct; /* the persistent kernels of the call (chunk
