@@ -45,8 +45,8 @@ struct Lane {
   void* arena_mem = nullptr;
   cudaStream_t stream = nullptr;
   std::thread th;
-  uint64_t batches = 0;
-  bool busy = false;       // a range lane with a batch on the GPU
+  std::atomic<uint64_t> batches{0};  // read by gb_serve_stats_get from other threads
+  bool busy = false;       // a range lane with a batch on the GPU (under the server mutex)
 };
 
 // First-fit allocator over one device allocation (host-side bookkeeping,

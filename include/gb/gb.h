@@ -98,7 +98,9 @@ typedef struct gb_range_opts {
   uint64_t phase2_limit;  /* Phase-2 bound (0: 1e8); n with no p <=
                              max(p_small, phase2_limit) is a failure       */
   uint32_t chunk_evens;   /* even n per CTA window (0: auto; power of 2,
-                             2^12..2^20)                                   */
+                             2^13..2^20; at most 2^16 when min_p is asked
+                             for: each n's entry is kept in shared memory
+                             until the chunk writes the minimal p out)     */
   uint32_t halo;          /* q-window halo in numbers (0: auto; multiple of
                              64, 128..2^17); primes p < halo are searched
                              in shared memory, larger ones on the Phase-2
