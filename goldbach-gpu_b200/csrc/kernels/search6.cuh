@@ -58,7 +58,9 @@ constexpr int kLevels6 = 4;
 __host__ __device__ constexpr uint32_t level6_start(int l) {
   return l == 0 ? 0u : l == 1 ? 28u : l == 2 ? 40u : 56u;
 }
-constexpr int kWT6 = 7;                      // U words per lane per warp task
+constexpr int kWT6 = 8;                      // U words per lane per warp task (6: 587.7,
+                                             // 7: 601.0, 8: 562.5, 9: 570.0, 10: 585.1,
+                                             // 12: 656.4 ms on [4, 1e12])
 constexpr uint32_t kTaskWords6 = 32 * kWT6;  // words per warp task
 
 // Per-CTA search context (static shared memory): the class tables' lengths
@@ -326,7 +328,7 @@ __device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_
   const uint32_t pos0 = level6_start(L), pend = level6_end(ri, L);
   if constexpr (!MINP && !LISTED) {
     // Level 0 steps in pairs (its span starts at entry 0): the two
-    // steps' counts, at most 7 * 32 * 32 = 7168 each, share one warp
+    // steps' counts, at most kWT6 * 32 * 32 = 8192 each, share one warp
     // reduction packed in the halves of a word, and the early-exit vote
     // comes every fourth pair.  Each step clears the q-prime bits of the
     // lane's words and counts the lane's unresolved n: resolved = live
@@ -404,7 +406,7 @@ __device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_
         cnt = live - now;
         live = now;
       }
-      // two steps' counts (at most 7 * 32 * 32 = 7168 each) share one warp
+      // two steps' counts (at most kWT6 * 32 * 32 = 8192 each) share one warp
       // reduction, packed in the two halves of a word
       if (pending) {
         const uint32_t v = __reduce_add_sync(0xffffffffu, held | (cnt << 16));
