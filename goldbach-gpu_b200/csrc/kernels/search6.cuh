@@ -43,20 +43,21 @@ constexpr uint32_t kLockSteps6 = 256;  // table stride of each class sequence
 constexpr uint32_t kLockEntries6 = kLockSteps6 - 1;
 
 // The lockstep runs in levels: level 0 takes every word of the chunk through
-// the entries [0, 28); each later level takes the words still holding an
+// the entries [0, 32); each later level takes the words still holding an
 // unresolved n (a per-class survivor list written by the level before it,
 // densely packed) through its own span, and the last level runs to the end
 // of the table.  A word costs the steps of the task it sits in (a task ends
 // when all its words are resolved), so re-packing the survivors keeps the
-// slow words together: near 1e12 the words alive after 28, 40 and 56
-// entries are about 45%, 17% and 3.7%, and the levels take about 0.76 of
-// the word-steps of a single split at 40 entries (measured: 1.50 against
-// 1.55 ms for 2^30 even n near 1e12; the barrier between levels and the
-// survivor traffic take the rest; 3, 5 and 7 levels measured 1.51, 1.50
-// and 1.56 ms).
+// slow words together: near 1e12 about 45%, 17% and 3.7% of the words are
+// still alive after 28, 40 and 56 entries, and four levels took about 0.76
+// of the word-steps of a single split at 40 entries (1.50 against 1.55 ms
+// for 2^30 even n near 1e12; 3, 5 and 7 levels measured 1.51, 1.50 and
+// 1.56 ms).  Level starts with 8 words per lane, on [4, 1e12]: (32, 44, 60)
+// 557.6 ms; (28, 40, 56) 562.7; (36, 48, 64) 560.7; (32, 48, 64) 559.8;
+// (24, 36, 52) 568.7; (40, 52, 68) 568.4; (20, 32, 48) 582.7.
 constexpr int kLevels6 = 4;
 __host__ __device__ constexpr uint32_t level6_start(int l) {
-  return l == 0 ? 0u : l == 1 ? 28u : l == 2 ? 40u : 56u;
+  return l == 0 ? 0u : l == 1 ? 32u : l == 2 ? 44u : 60u;
 }
 constexpr int kWT6 = 8;                      // U words per lane per warp task (6: 587.7,
                                              // 7: 601.0, 8: 562.5, 9: 570.0, 10: 585.1,
