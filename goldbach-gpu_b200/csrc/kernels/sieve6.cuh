@@ -59,6 +59,22 @@ __device__ __forceinline__ uint32_t base_mod(int64_t G0, uint32_t p, uint64_t ma
   return m ? p - m : 0;
 }
 
+// floor(sqrt(x)), at most 2^32 - 1.
+__device__ __forceinline__ uint32_t isqrt64(uint64_t x) {
+  uint64_t r = (uint64_t)sqrt((double)x);
+  if (r > 0xffffffffull) r = 0xffffffffull;
+  while (r * r > x) --r;
+  while (r < 0xffffffffull && (r + 1) * (r + 1) <= x) ++r;
+  return (uint32_t)r;
+}
+
+// First marks of both classes, for a window that starts at or above
+// p^2 + 4 (first_marks6's short path, unclamped): both < p.
+__device__ __forceinline__ void near_marks6(uint32_t p, uint2 ac, uint32_t r, uint32_t& t1, uint32_t& t5) {
+  t1 = ac.x >= r ? ac.x - r : ac.x + p - r;
+  t5 = ac.y >= r ? ac.y - r : ac.y + p - r;
+}
+
 // Sieves bits [0, nbits) of both class bitsets (nwords words each written).
 // Exact for every q <= q_top.  pat6: the class wheel patterns (shared
 // memory).  primes[kWheelPrimeCount+1 .. nsieve) are the marking primes
@@ -138,6 +154,11 @@ __device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ 
   //    (stride 32p stays far below 2^32: these primes are < nbits / 64).
   const uint32_t kfirst = kWheelPrimeCount + 1;
   const uint32_t kc = kcoop < nsieve ? kcoop : nsieve;
+  // the window's prime bounds, in 32 bits: p <= plim <=> p^2 <= q_top, and
+  // p <= psafe <=> the window starts at or above p^2 + 4 (the short path
+  // of the first marks)
+  const uint32_t plim = isqrt64(q_top);
+  const uint32_t psafe = G0 >= 1 ? isqrt64(6 * (uint64_t)G0 - 4) : 0u;
   {  // the next prime's table entries are loaded one iteration ahead
     uint32_t k = kfirst + warp;
     uint32_t pn = 0;
@@ -149,9 +170,10 @@ __device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ 
       const uint64_t mg = mn;
       const uint2 ac = an;
       if (k + NW < kc) { pn = __ldg(primes + k + NW); mn = __ldg(magic + k + NW); an = __ldg(a15 + k + NW); }
-      if ((uint64_t)p * p > q_top) break;
+      if (p > plim) break;
       uint32_t t1, t5;
-      first_marks6(G0, p, ac, base_mod(G0, p, mg), nbits, t1, t5);
+      if (p <= psafe) near_marks6(p, ac, base_mod(G0, p, mg), t1, t5);
+      else first_marks6(G0, p, ac, base_mod(G0, p, mg), nbits, t1, t5);
       const uint32_t stride = 32 * p;
       for (uint32_t i = t1 + lane * p; i < nbits; i += stride)
         atomicAnd(&Q1[i >> 5], ~(1u << (i & 31)));
@@ -172,9 +194,10 @@ __device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ 
       const uint64_t mg = mn;
       const uint2 ac = an;
       if (k + NT < nsieve) { pn = __ldg(primes + k + NT); mn = __ldg(magic + k + NT); an = __ldg(a15 + k + NT); }
-      if ((uint64_t)p * p > q_top) break;
-      uint32_t j1, j5;
-      first_marks6(G0, p, ac, base_mod(G0, p, mg), nbits, j1, j5);
+      if (p > plim) break;
+      uint32_t j1, j5;  // offsets >= nbits mean no mark
+      if (p <= psafe) near_marks6(p, ac, base_mod(G0, p, mg), j1, j5);
+      else first_marks6(G0, p, ac, base_mod(G0, p, mg), nbits, j1, j5);
       if (p >= nbits) {  // at most one multiple per class: no loop (no divergent exits)
         if (j1 < nbits) atomicAnd(&Q1[j1 >> 5], ~(1u << (j1 & 31)));
         if (j5 < nbits) atomicAnd(&Q5[j5 >> 5], ~(1u << (j5 & 31)));
