@@ -68,6 +68,19 @@ __device__ __forceinline__ uint32_t isqrt64(uint64_t x) {
   return (uint32_t)r;
 }
 
+// r = G0 mod p from a double-precision quotient estimate, for 0 <= G0 <
+// 2^53 and p < 2^31; gs = G0 / 2^64 (exact), gl = G0 mod 2^32.  With
+// magic = floor((2^64 - 1) / p), G0 magic / 2^64 is within 2 G0 / 2^64 of
+// G0 / p, and rounding magic to a double adds G0 / p * 2^-53 at most, so the
+// estimate is within 1/4 of G0 / p; adding 1.5 * 2^52 rounds it to
+// floor(G0 / p) or one more, held in the double's low bits.  G0 - p q then
+// lies in (-p, p), and 32-bit arithmetic finishes it.
+__device__ __forceinline__ uint32_t near_mod(double gs, uint32_t gl, uint32_t p, uint64_t magic) {
+  const double est = fma(gs, __ull2double_rn(magic), 6755399441055744.0);  // + 1.5 * 2^52
+  const uint32_t r = gl - (uint32_t)__double_as_longlong(est) * p;
+  return min(r, r + p);
+}
+
 // First marks of both classes, for a window that starts at or above
 // p^2 + 4 (first_marks6's short path, unclamped): both < p.
 __device__ __forceinline__ void near_marks6(uint32_t p, uint2 ac, uint32_t r, uint32_t& t1, uint32_t& t5) {
@@ -159,6 +172,11 @@ __device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ 
   // of the first marks)
   const uint32_t plim = isqrt64(q_top);
   const uint32_t psafe = G0 >= 1 ? isqrt64(6 * (uint64_t)G0 - 4) : 0u;
+  // r = G0 mod p by the quotient estimate where the window allows it
+  // (every prime used is <= plim)
+  const bool fastr = G0 >= 0 && G0 < (1ll << 53) && plim < 0x80000000u;
+  const double gs = (double)G0 * 0x1p-64;
+  const uint32_t gl = (uint32_t)G0;
   {  // the next prime's table entries are loaded one iteration ahead
     uint32_t k = kfirst + warp;
     uint32_t pn = 0;
@@ -172,8 +190,9 @@ __device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ 
       if (k + NW < kc) { pn = __ldg(primes + k + NW); mn = __ldg(magic + k + NW); an = __ldg(a15 + k + NW); }
       if (p > plim) break;
       uint32_t t1, t5;
-      if (p <= psafe) near_marks6(p, ac, base_mod(G0, p, mg), t1, t5);
-      else first_marks6(G0, p, ac, base_mod(G0, p, mg), nbits, t1, t5);
+      const uint32_t r = fastr ? near_mod(gs, gl, p, mg) : base_mod(G0, p, mg);
+      if (p <= psafe) near_marks6(p, ac, r, t1, t5);
+      else first_marks6(G0, p, ac, r, nbits, t1, t5);
       const uint32_t stride = 32 * p;
       for (uint32_t i = t1 + lane * p; i < nbits; i += stride)
         atomicAnd(&Q1[i >> 5], ~(1u << (i & 31)));
@@ -196,8 +215,9 @@ __device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ 
       if (k + NT < nsieve) { pn = __ldg(primes + k + NT); mn = __ldg(magic + k + NT); an = __ldg(a15 + k + NT); }
       if (p > plim) break;
       uint32_t j1, j5;  // offsets >= nbits mean no mark
-      if (p <= psafe) near_marks6(p, ac, base_mod(G0, p, mg), j1, j5);
-      else first_marks6(G0, p, ac, base_mod(G0, p, mg), nbits, j1, j5);
+      const uint32_t r = fastr ? near_mod(gs, gl, p, mg) : base_mod(G0, p, mg);
+      if (p <= psafe) near_marks6(p, ac, r, j1, j5);
+      else first_marks6(G0, p, ac, r, nbits, j1, j5);
       if (p >= nbits) {  // at most one multiple per class: no loop (no divergent exits)
         if (j1 < nbits) atomicAnd(&Q1[j1 >> 5], ~(1u << (j1 & 31)));
         if (j5 < nbits) atomicAnd(&Q5[j5 >> 5], ~(1u << (j5 & 31)));
