@@ -88,6 +88,26 @@ __device__ __forceinline__ void near_marks6(uint32_t p, uint2 ac, uint32_t r, ui
   t5 = ac.y >= r ? ac.y - r : ac.y + p - r;
 }
 
+// First marks t1, t5 of p in the window (>= nbits: none below it).  fastr:
+// the window allows near_mod (p < 2^31 for every p used); near: p <= the
+// window's psafe, so both offsets are below p.  With both, each offset is
+// a - r wrapped into [0, p) by one unsigned min (a - r + p < 2^32).
+__device__ __forceinline__ void window_marks6(bool fastr, bool near, double gs, uint32_t gl, int64_t G0,
+                                              uint32_t p, uint64_t mg, uint2 ac, uint32_t nbits,
+                                              uint32_t& t1, uint32_t& t5) {
+  if (fastr && near) {
+    const uint32_t r = near_mod(gs, gl, p, mg);
+    t1 = ac.x - r;
+    t1 = min(t1, t1 + p);
+    t5 = ac.y - r;
+    t5 = min(t5, t5 + p);
+    return;
+  }
+  const uint32_t r = fastr ? near_mod(gs, gl, p, mg) : base_mod(G0, p, mg);
+  if (near) near_marks6(p, ac, r, t1, t5);
+  else first_marks6(G0, p, ac, r, nbits, t1, t5);
+}
+
 // Sieves bits [0, nbits) of both class bitsets (nwords words each written).
 // Exact for every q <= q_top.  pat6: the class wheel patterns (shared
 // memory).  primes[kWheelPrimeCount+1 .. nsieve) are the marking primes
@@ -190,9 +210,7 @@ __device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ 
       if (k + NW < kc) { pn = __ldg(primes + k + NW); mn = __ldg(magic + k + NW); an = __ldg(a15 + k + NW); }
       if (p > plim) break;
       uint32_t t1, t5;
-      const uint32_t r = fastr ? near_mod(gs, gl, p, mg) : base_mod(G0, p, mg);
-      if (p <= psafe) near_marks6(p, ac, r, t1, t5);
-      else first_marks6(G0, p, ac, r, nbits, t1, t5);
+      window_marks6(fastr, p <= psafe, gs, gl, G0, p, mg, ac, nbits, t1, t5);
       const uint32_t stride = 32 * p;
       for (uint32_t i = t1 + lane * p; i < nbits; i += stride)
         atomicAnd(&Q1[i >> 5], ~(1u << (i & 31)));
@@ -215,9 +233,7 @@ __device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ 
       if (k + NT < nsieve) { pn = __ldg(primes + k + NT); mn = __ldg(magic + k + NT); an = __ldg(a15 + k + NT); }
       if (p > plim) break;
       uint32_t j1, j5;  // offsets >= nbits mean no mark
-      const uint32_t r = fastr ? near_mod(gs, gl, p, mg) : base_mod(G0, p, mg);
-      if (p <= psafe) near_marks6(p, ac, r, j1, j5);
-      else first_marks6(G0, p, ac, r, nbits, j1, j5);
+      window_marks6(fastr, p <= psafe, gs, gl, G0, p, mg, ac, nbits, j1, j5);
       if (p >= nbits) {  // at most one multiple per class: no loop (no divergent exits)
         if (j1 < nbits) atomicAnd(&Q1[j1 >> 5], ~(1u << (j1 & 31)));
         if (j5 < nbits) atomicAnd(&Q5[j5 >> 5], ~(1u << (j5 & 31)));
