@@ -9,8 +9,9 @@
 // Each prime p >= 5 has one multiple in every 6p numbers per class, so in
 // both bitsets its multiples are p bits apart: the sieve marks 2/3 of the
 // bits it would mark odd-only.  The first multiple in a window costs one
-// Barrett reduction r = G0 mod p for both classes, using the per-prime class
-// offsets a1 = -1/6 and a5 = -5/6 (mod p) kept with the prime table:
+// reduction r = G0 mod p for both classes (a double-precision quotient
+// estimate where the window allows it, else Barrett), using the per-prime
+// class offsets a1 = -1/6 and a5 = -5/6 (mod p) kept with the prime table:
 //     6(G0+t) + c == 0 (mod p)  <=>  t == a_c - r (mod p).
 #pragma once
 #include "../gb_device.cuh"
@@ -153,7 +154,7 @@ __device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ 
         const uint32_t* pp = pat6 + wheel6_offset(cls5, x) + (rr >> 5);
         w &= __funnelshift_r(pp[0], pp[1], rr & 31);
         const uint32_t nr = rr + step;
-        r[x] = nr >= P ? nr - P : nr;
+        r[x] = min(nr, nr - P);  // nr - P wraps above nr when nr < P
       }
       if (L1) {
         const uint32_t* L = cls5 ? L5 : L1;
@@ -218,8 +219,8 @@ __device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ 
         atomicAnd(&Q5[i >> 5], ~(1u << (i & 31)));
     }
   }
-  // 4. one thread per prime for the rest, both classes in one loop; the
-  //    steps are taken only while they stay below nbits (p may be near 2^32).
+  // 4. one thread per prime for the rest, both classes in one loop; primes
+  //    >= nbits (possibly near 2^32) take a loop-free body.
   {  // the next prime's table entries are loaded one iteration ahead
     uint32_t k = (kc > kfirst ? kc : kfirst) + tid;
     uint32_t pn = 0;
@@ -239,14 +240,15 @@ __device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ 
         if (j5 < nbits) atomicAnd(&Q5[j5 >> 5], ~(1u << (j5 & 31)));
         continue;
       }
+      // p < nbits here: j + p stays below 2 nbits < 2^32
       while (j1 < nbits || j5 < nbits) {
         if (j1 < nbits) {
           atomicAnd(&Q1[j1 >> 5], ~(1u << (j1 & 31)));
-          j1 = nbits - j1 > p ? j1 + p : nbits;
+          j1 += p;
         }
         if (j5 < nbits) {
           atomicAnd(&Q5[j5 >> 5], ~(1u << (j5 & 31)));
-          j5 = nbits - j5 > p ? j5 + p : nbits;
+          j5 += p;
         }
       }
     }
