@@ -131,12 +131,13 @@ __device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ 
   const int warp = tid >> 5;
   constexpr int NW = NT / 32;
 
-  // 1. wheel fill of both classes: word t covers G0 + 32t .. +31.
+  // 1. wheel fill of both classes: each thread builds words t and t + 1
+  //    (G0 + 32t .. +63) per step, from three pattern words per group.
 #pragma unroll
   for (int cls5 = 0; cls5 < 2; ++cls5) {
     uint32_t* Q = cls5 ? Q5 : Q1;
     uint32_t r[kWheel6Groups];
-    const int64_t g = G0 + 32 * (int64_t)tid;
+    const int64_t g = G0 + 64 * (int64_t)tid;
 #pragma unroll
     for (int x = 0; x < kWheel6Groups; ++x) {
       const int64_t P = wheel6_period(x);
@@ -144,23 +145,30 @@ __device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ 
       if (m < 0) m += P;
       r[x] = (uint32_t)m;
     }
-    for (uint32_t t = tid; t < nwords; t += NT) {
-      uint32_t w = 0xffffffffu;
+    for (uint32_t t = 2 * tid; t < nwords; t += 2 * NT) {
+      uint32_t w0 = 0xffffffffu, w1 = 0xffffffffu;
 #pragma unroll
       for (int x = 0; x < kWheel6Groups; ++x) {
         const uint32_t P = wheel6_period(x);
-        const uint32_t step = (uint32_t)((32ull * NT) % P);
+        const uint32_t step = (uint32_t)((64ull * NT) % P);
         const uint32_t rr = r[x];
+        // bits [rr, rr + 64) of the pattern, which is stored to P + 64
         const uint32_t* pp = pat6 + wheel6_offset(cls5, x) + (rr >> 5);
-        w &= __funnelshift_r(pp[0], pp[1], rr & 31);
+        const uint32_t a = pp[0], b = pp[1], c = pp[2];
+        w0 &= __funnelshift_r(a, b, rr & 31);
+        w1 &= __funnelshift_r(b, c, rr & 31);
         const uint32_t nr = rr + step;
         r[x] = min(nr, nr - P);  // nr - P wraps above nr when nr < P
       }
-      if (L1) {
+      const bool two = t + 1 < nwords;
+      if (L1) {  // the mask holds nwords + 1 words: word t + 2 only when t + 1 is in
         const uint32_t* L = cls5 ? L5 : L1;
-        w &= __funnelshift_r(__ldg(L + t), __ldg(L + t + 1), lsh);
+        const uint32_t l1 = __ldg(L + t + 1);
+        w0 &= __funnelshift_r(__ldg(L + t), l1, lsh);
+        if (two) w1 &= __funnelshift_r(l1, __ldg(L + t + 2), lsh);
       }
-      Q[t] = w;
+      Q[t] = w0;
+      if (two) Q[t + 1] = w1;
     }
   }
   __syncthreads();
@@ -213,8 +221,10 @@ __device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ 
       uint32_t t1, t5;
       window_marks6(fastr, p <= psafe, gs, gl, G0, p, mg, ac, nbits, t1, t5);
       const uint32_t stride = 32 * p;
+#pragma unroll 4
       for (uint32_t i = t1 + lane * p; i < nbits; i += stride)
         atomicAnd(&Q1[i >> 5], ~(1u << (i & 31)));
+#pragma unroll 4
       for (uint32_t i = t5 + lane * p; i < nbits; i += stride)
         atomicAnd(&Q5[i >> 5], ~(1u << (i & 31)));
     }
