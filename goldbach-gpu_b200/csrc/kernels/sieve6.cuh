@@ -221,10 +221,10 @@ __device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ 
       uint32_t t1, t5;
       window_marks6(fastr, p <= psafe, gs, gl, G0, p, mg, ac, nbits, t1, t5);
       const uint32_t stride = 32 * p;
-#pragma unroll 4
+#pragma unroll 8
       for (uint32_t i = t1 + lane * p; i < nbits; i += stride)
         atomicAnd(&Q1[i >> 5], ~(1u << (i & 31)));
-#pragma unroll 4
+#pragma unroll 8
       for (uint32_t i = t5 + lane * p; i < nbits; i += stride)
         atomicAnd(&Q5[i >> 5], ~(1u << (i & 31)));
     }
@@ -251,14 +251,17 @@ __device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ 
         continue;
       }
       // p < nbits here: j + p stays below 2 nbits < 2^32
-      while (j1 < nbits || j5 < nbits) {
-        if (j1 < nbits) {
-          atomicAnd(&Q1[j1 >> 5], ~(1u << (j1 & 31)));
-          j1 += p;
-        }
-        if (j5 < nbits) {
-          atomicAnd(&Q5[j5 >> 5], ~(1u << (j5 & 31)));
-          j5 += p;
+      while (j1 < nbits || j5 < nbits) {  // two marks per class per pass
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          if (j1 < nbits) {
+            atomicAnd(&Q1[j1 >> 5], ~(1u << (j1 & 31)));
+            j1 += p;
+          }
+          if (j5 < nbits) {
+            atomicAnd(&Q5[j5 >> 5], ~(1u << (j5 & 31)));
+            j5 += p;
+          }
         }
       }
     }
