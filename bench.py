@@ -47,9 +47,9 @@ UNIT = "even n/s"
 #  * one first-multiple reduction (8 ALU ops) per sieving prime per chunk.
 SEARCH_TESTS_PER_N = 14.85
 # DRAM bytes of range6_kernel per even n: one ncu capture of 2^30 even n
-# ending at 1e12 read 1.96 MB and wrote 12.63 MB (the search's survivor
+# ending at 1e12 read 1.97 MB and wrote 13.51 MB (the search's survivor
 # lists spilling out of L2, the prime tables' first touch)
-DRAM_BYTES_PER_N = (1.963520e6 + 12.630016e6) / 2**30
+DRAM_BYTES_PER_N = (1.972480e6 + 13.508352e6) / 2**30
 SEARCH_OPS_PER_WORD = 5
 WHEEL_OPS_PER_ODD_Q = 14 / 32
 MARKS_PER_ODD_Q = 1.1225
@@ -781,7 +781,7 @@ def main():
             "bound": "int", "achieved": achieved / 1e12, "peak": alu_peak / 1e12, "unit": "Top/s",
             "frac": achieved / alu_peak, "traffic": DRAM_BYTES_PER_N * n_mine,
             "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of range6_kernel "
-                               "on 2^30 even n ending at 1e12 (14.6 MB), scaled by the n of the "
+                               "on 2^30 even n ending at 1e12 (15.5 MB), scaled by the n of the "
                                "launch (the survivor lists' spill out of L2 grows with n)"),
             "kernel": "range6_kernel", "kernel_ms": k_s * 1e3,
             "peak_source": "measured in-process: gb_probe_peaks (32-bit ALU ops/s; shared-memory atomicAnd/s)",
