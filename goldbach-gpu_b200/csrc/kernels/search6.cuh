@@ -59,6 +59,9 @@ constexpr int kLevels6 = 4;
 __host__ __device__ constexpr uint32_t level6_start(int l) {
   return l == 0 ? 0u : l == 1 ? 32u : l == 2 ? 44u : 60u;
 }
+// the paired steps load two entries at an even position with one 8-byte load
+static_assert(level6_start(1) % 2 == 0 && level6_start(2) % 2 == 0 && level6_start(3) % 2 == 0,
+              "level starts must be even");
 constexpr int kWT6 = 8;                      // U words per lane per warp task (6: 587.7,
                                              // 7: 601.0, 8: 562.5, 9: 570.0, 10: 585.1,
                                              // 12: 656.4 ms on [4, 1e12])
@@ -327,8 +330,9 @@ __device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_
     for (int i = 0; i < kWT6; ++i) live += __popc(U[i]);
   }
   const uint32_t pos0 = level6_start(L), pend = level6_end(ri, L);
-  if constexpr (!MINP && !LISTED) {
-    // Level 0 steps in pairs (its span starts at entry 0): the two
+  if constexpr (!MINP) {
+    // Without per-n output every level steps in pairs (its span starts at
+    // an even entry: 0, 32, 44 or 60): the two
     // steps' counts, at most kWT6 * 32 * 32 = 8192 each, share one warp
     // reduction packed in the halves of a word, and the early-exit vote
     // comes every fourth pair.  Each step clears the q-prime bits of the

@@ -221,10 +221,10 @@ __device__ void sieve_window6(uint32_t* __restrict__ Q1, uint32_t* __restrict__ 
       uint32_t t1, t5;
       window_marks6(fastr, p <= psafe, gs, gl, G0, p, mg, ac, nbits, t1, t5);
       const uint32_t stride = 32 * p;
-#pragma unroll 8
+#pragma unroll 16
       for (uint32_t i = t1 + lane * p; i < nbits; i += stride)
         atomicAnd(&Q1[i >> 5], ~(1u << (i & 31)));
-#pragma unroll 8
+#pragma unroll 16
       for (uint32_t i = t5 + lane * p; i < nbits; i += stride)
         atomicAnd(&Q5[i >> 5], ~(1u << (i & 31)));
     }
