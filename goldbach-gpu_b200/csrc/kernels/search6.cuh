@@ -64,7 +64,9 @@ static_assert(level6_start(1) % 2 == 0 && level6_start(2) % 2 == 0 && level6_sta
               "level starts must be even");
 constexpr int kWT6 = 8;                      // U words per lane per warp task (6: 587.7,
                                              // 7: 601.0, 8: 562.5, 9: 570.0, 10: 585.1,
-                                             // 12: 656.4 ms on [4, 1e12])
+                                             // 12: 656.4 ms on [4, 1e12]; with the
+                                             // paired levels and the faster sieve,
+                                             // 7: 449.7, 8: 436.9, 9: 437.9 ms)
 constexpr uint32_t kTaskWords6 = 32 * kWT6;  // words per warp task
 
 // Per-CTA search context (static shared memory): the class tables' lengths
