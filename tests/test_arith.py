@@ -3,6 +3,12 @@ on the CPU (the GPU tests check the device code against the oracle):
 
 * the double-precision quotient estimate of mod_p_f64 (gb_device.cuh):
   within 1 of floor(x / p) whenever x / p < 2^51;
+* the sieve's G0 mod p from one FMA of G0 / 2^64 by the Barrett magic as
+  a double (near_mod, kernels/sieve6.cuh), for 0 <= G0 < 2^53, p < 2^31;
+* the windows' large-prime remainder from one FMA of g0 (a double) by a
+  reciprocal built from the single-precision one and a Newton step
+  (large_prime / large_pair, kernels/windows.cu), for g0 < 2^62,
+  2^20 < p < 2^31;
 * the 32-bit-limb Montgomery product of mont_mul32 (gb_device.cuh), step by
   step with its carries, against a * b * 2^-64 mod n;
 * R mod n without division (mont32_init, kernels/single.cu) and the
@@ -11,6 +17,9 @@ on the CPU (the GPU tests check the device code against the oracle):
   x * r^-1 mod 2^32 <= (2^32 - 1) / r for odd r.
 """
 import random
+from fractions import Fraction
+
+import numpy as np
 
 M32 = (1 << 32) - 1
 
@@ -29,6 +38,46 @@ def test_double_quotient_estimate_within_one():
         assert abs(q - x // p) <= 1
         r = x - q * p
         assert -p < r < 2 * p
+
+
+def _fma(a, b, c):
+    """a * b + c with one rounding to the nearest double."""
+    return float(Fraction(a) * Fraction(b) + Fraction(c))
+
+
+def _low32_of_rounded(est):
+    """The low 32 bits of the integer held by a double in [2^52, 2^53)."""
+    assert 2.0**52 <= est < 2.0**53
+    return int(est) & M32
+
+
+def test_sieve_remainder_from_the_barrett_magic_as_a_double():
+    rng = random.Random(11)
+    for _ in range(20000):
+        p = rng.choice([71, 73, 1009, 999983, (1 << 31) - 1, rng.randrange(71, 1 << 31) | 1])
+        g0 = rng.choice([rng.randrange(0, 1 << 53), rng.randrange(0, 1 << 40),
+                         (rng.randrange(0, (1 << 53) // p) * p + rng.choice([0, 1, p - 1])) % (1 << 53)])
+        magic = ((1 << 64) - 1) // p
+        est = _fma(g0 * 2.0**-64, float(magic), 1.5 * 2.0**52)
+        r = (g0 - _low32_of_rounded(est) * p) & M32
+        r = min(r, (r + p) & M32)
+        assert r == g0 % p, (g0, p)
+
+
+def test_window_remainder_from_the_newton_reciprocal():
+    rng = random.Random(13)
+    for _ in range(20000):
+        p = rng.choice([(1 << 20) + 7, (1 << 31) - 1, rng.randrange((1 << 20) + 1, 1 << 31) | 1])
+        g0 = rng.choice([rng.randrange(1 << 30, 1 << 62), (1 << 62) - 1 - rng.randrange(1 << 20),
+                         p * rng.randrange(1, ((1 << 62) - 1) // p) + rng.choice([0, 1, p - 1])])
+        g0 = min(g0, (1 << 62) - 1)
+        pd = float(p)
+        r0 = float(np.float32(1.0) / np.float32(p))  # __frcp_rn((float)p)
+        inv = _fma(r0, _fma(-pd, r0, 1.0), r0)
+        est = _fma(float(g0), inv, 1.5 * 2.0**52)
+        r = (g0 - _low32_of_rounded(est) * p) & M32
+        r = min(r, (r + p) & M32)
+        assert r == g0 % p, (g0, p)
 
 
 def _mont_mul32(a, b, n, ninv0):
