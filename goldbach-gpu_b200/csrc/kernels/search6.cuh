@@ -334,12 +334,11 @@ __device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_
   const uint32_t pos0 = level6_start(L), pend = level6_end(ri, L);
   if constexpr (!MINP) {
     // Without per-n output every level steps in pairs (its span starts at
-    // an even entry: 0, 32, 44 or 60): the two
-    // steps' counts, at most kWT6 * 32 * 32 = 8192 each, share one warp
-    // reduction packed in the halves of a word, and the early-exit vote
-    // comes every fourth pair.  Each step clears the q-prime bits of the
-    // lane's words and counts the lane's unresolved n: resolved = live
-    // before - live after.
+    // an even entry: 0, 32, 44 or 60): the two steps' counts, at most
+    // kWT6 * 32 * 32 = 8192 each, share one warp reduction packed in the
+    // halves of a word, and the early-exit vote comes every fourth pair.
+    // Each step clears the q-prime bits of the lane's words and counts the
+    // lane's unresolved n: resolved = live before - live after.
     auto step = [&](uint32_t e) -> uint32_t {
       const uint32_t q5 = e >> 31;
       const uint32_t off = (q5 ? K5 : K1) - e6_u(e);
@@ -383,7 +382,7 @@ __device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_
       const uint32_t v = __reduce_add_sync(0xffffffffu, step(e));
       if (lane == 0 && v) atomicAdd(&HIST[e6_k(e)], v);
     }
-  } else {
+  } else {  // per-n output: one step at a time, each recording its entry position
     uint32_t held = 0, kheld = 0;  // a step's count waiting for the next step's
     bool pending = false;          // (warp-uniform)
 #pragma unroll 1
@@ -399,20 +398,7 @@ __device__ __noinline__ void search_task6(const SearchParams& s, int ri, uint32_
       const uint32_t off = (q5 ? K5 : K1) - e6_u(e);
       const uint32_t wo = off >> 5;
       ca.at(q5 ? Q5 : Q1, wo, wo | (q5 << 31), W);
-      uint32_t cnt;
-      if (MINP) {
-        cnt = step6<MINP, kWT6>(U, ca.lo, ca.hi, off & 31, pos, W, jbase);
-      } else {  // clear and count the lane's unresolved n (live before - after)
-        uint32_t now = 0;
-        const uint32_t sh = off & 31;
-#pragma unroll
-        for (int i = 0; i < kWT6; ++i) {
-          U[i] &= ~__funnelshift_r(ca.lo[i], ca.hi[i], sh);
-          now += __popc(U[i]);
-        }
-        cnt = live - now;
-        live = now;
-      }
+      const uint32_t cnt = step6<MINP, kWT6>(U, ca.lo, ca.hi, off & 31, pos, W, jbase);
       // two steps' counts (at most kWT6 * 32 * 32 = 8192 each) share one warp
       // reduction, packed in the two halves of a word
       if (pending) {
