@@ -29,6 +29,7 @@
 #include <unordered_map>
 
 #include "gb_ctx.h"
+#include "latency_hist.h"
 
 using namespace gb;
 
@@ -136,7 +137,7 @@ struct gb_server {
   unsigned long long* h_agg = nullptr;
   bool single_graph = false;  // the single lane runs its small batches as a graph
   // stats
-  std::vector<double> lat;
+  LatencyHist lat;  // completed requests' latencies since start or the last reset
   uint64_t submitted = 0, completed = 0, rejected = 0, busy = 0, t0 = 0;
 };
 
@@ -154,7 +155,7 @@ void finish(gb_server* S, const Pending& p, gb_response& resp, uint64_t t_done) 
   std::lock_guard<std::mutex> lk(S->mu);
   S->done[p.ticket] = resp;
   S->completed++;
-  if (resp.status == GB_OK) S->lat.push_back(resp.latency_us);
+  if (resp.status == GB_OK) S->lat.add(resp.latency_us);
   S->cv_done.notify_all();
 }
 
@@ -646,17 +647,12 @@ gb_status gb_serve_stats_get(gb_ctx* c, gb_serve_stats* out, int reset) {
   out->pool_bytes = S->pool.cap;
   out->pool_peak_bytes = S->pool.peak;
   out->elapsed_s = (now_ns() - S->t0) / 1e9;
-  if (!S->lat.empty()) {
-    std::vector<double> v = S->lat;
-    std::sort(v.begin(), v.end());
-    auto pct = [&](double f) { return v[std::min<size_t>(v.size() - 1, (size_t)(f * (v.size() - 1) + 0.5))]; };
-    out->p50_us = pct(0.50);
-    out->p99_us = pct(0.99);
-    out->max_us = v.back();
-    double s = 0;
-    for (double x : v) s += x;
-    out->mean_us = s / v.size();
-    out->completed_per_s = v.size() / std::max(out->elapsed_s, 1e-9);
+  if (S->lat.count()) {
+    out->p50_us = S->lat.quantile(0.50);
+    out->p99_us = S->lat.quantile(0.99);
+    out->max_us = S->lat.max();
+    out->mean_us = S->lat.mean();
+    out->completed_per_s = S->lat.count() / std::max(out->elapsed_s, 1e-9);
   }
   if (reset) {
     S->lat.clear();
