@@ -623,7 +623,11 @@ gb_status gb_wait(gb_ctx* c, uint64_t ticket, gb_response* out, uint64_t timeout
   if (!c || !c->server || !out) return GB_EINVAL;
   gb_server* S = c->server;
   std::unique_lock<std::mutex> lk(S->mu);
-  const bool got = S->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] {
+  if (!ticket || ticket >= S->next_ticket) return GB_EINVAL;  // never issued
+  // capped at 2^40 ms (about 35 years), so that UINT64_MAX ("no bound") fits
+  // the clock arithmetic of the wait instead of wrapping to a negative time
+  const uint64_t ms = std::min<uint64_t>(timeout_ms, 1ull << 40);
+  const bool got = S->cv_done.wait_for(lk, std::chrono::milliseconds((int64_t)ms), [&] {
     return S->done.count(ticket) != 0;
   });
   if (!got) return GB_ETIMEOUT;

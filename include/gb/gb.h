@@ -465,7 +465,9 @@ gb_status gb_submit(gb_ctx* ctx, const gb_request* reqs, size_t count, uint64_t*
 /* GB_OK and the response once done (the ticket is then released),
  * GB_EAGAIN while pending.  Thread-safe. */
 gb_status gb_poll(gb_ctx* ctx, uint64_t ticket, gb_response* out);
-/* Like gb_poll, waiting up to timeout_ms (GB_ETIMEOUT after that). */
+/* Like gb_poll, waiting up to timeout_ms (GB_ETIMEOUT after that; capped at
+ * 2^40 ms, so UINT64_MAX waits without a practical bound).  GB_EINVAL at
+ * once for a ticket that was never issued. */
 gb_status gb_wait(gb_ctx* ctx, uint64_t ticket, gb_response* out, uint64_t timeout_ms);
 /* Latency percentiles and throughput; reset != 0 starts a new window. */
 gb_status gb_serve_stats_get(gb_ctx* ctx, gb_serve_stats* out, int reset);
