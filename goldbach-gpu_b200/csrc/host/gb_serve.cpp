@@ -149,13 +149,19 @@ uint64_t range_bytes(const gb_request& r) {
   return windows_request_bytes(gb_window{r.a, r.count}, o);
 }
 
-void finish(gb_server* S, const Pending& p, gb_response& resp, uint64_t t_done) {
-  const uint64_t arr = p.r.arrival_ns;
-  resp.latency_us = t_done > arr ? (t_done - arr) / 1e3 : 0.0;
+// Records a batch's responses under one lock with one wake-up of the
+// waiting callers (a lock and a notify_all per request would wake every
+// gb_wait caller once per request of the batch).
+void finish_batch(gb_server* S, const std::vector<Pending>& take, std::vector<gb_response>& resp,
+                  uint64_t t_done) {
   std::lock_guard<std::mutex> lk(S->mu);
-  S->done[p.ticket] = resp;
-  S->completed++;
-  if (resp.status == GB_OK) S->lat.add(resp.latency_us);
+  for (size_t i = 0; i < take.size(); ++i) {
+    const uint64_t arr = take[i].r.arrival_ns;
+    resp[i].latency_us = t_done > arr ? (t_done - arr) / 1e3 : 0.0;
+    S->done[take[i].ticket] = resp[i];
+    S->completed++;
+    if (resp[i].status == GB_OK) S->lat.add(resp[i].latency_us);
+  }
   S->cv_done.notify_all();
 }
 
@@ -281,6 +287,7 @@ void single_lane(gb_server* S) {
   const bool graph = !S->o.no_graph && build_single_graph(S, B, base, &G);
   S->single_graph = graph;
   std::vector<Pending> take;
+  std::vector<gb_response> resps;
   for (;;) {
     take.clear();
     uint64_t total = 0;
@@ -331,8 +338,9 @@ void single_lane(gb_server* S) {
     chk(cudaStreamSynchronize(L.stream));
     const uint64_t t_done = now_ns();
     const uint32_t batch = (uint32_t)L.batches++;
+    resps.assign(take.size(), gb_response{});
     for (size_t i = 0; i < take.size(); ++i) {
-      gb_response resp{};
+      gb_response& resp = resps[i];
       resp.kind = take[i].r.kind;
       resp.lane = 0;
       resp.batch = batch;
@@ -347,8 +355,8 @@ void single_lane(gb_server* S) {
         resp.max_minp = S->h_agg[4 * i + 2];
         resp.minp_sum = S->h_agg[4 * i + 3];
       }
-      finish(S, take[i], resp, t_done);
     }
+    finish_batch(S, take, resps, t_done);
   }
 }
 
@@ -359,6 +367,7 @@ void range_lane(gb_server* S, int ln) {
   std::vector<Pending> take;
   std::vector<gb_window> win;
   std::vector<gb_window_result> res;
+  std::vector<gb_response> resps;
   for (;;) {
     take.clear();
     uint64_t off = 0, bytes = 0;
@@ -430,8 +439,9 @@ void range_lane(gb_server* S, int ln) {
       S->cv_work.notify_all();  // memory freed: a waiting lane may fit its batch now
     }
     const uint64_t t_done = now_ns();
+    resps.assign(take.size(), gb_response{});
     for (size_t i = 0; i < take.size(); ++i) {
-      gb_response resp{};
+      gb_response& resp = resps[i];
       resp.kind = GB_REQ_RANGE;
       resp.lane = (uint32_t)ln;
       resp.batch = batch;
@@ -442,8 +452,8 @@ void range_lane(gb_server* S, int ln) {
         resp.max_minp = res[i].max_minp;
         resp.minp_sum = res[i].minp_sum;
       }
-      finish(S, take[i], resp, t_done);
     }
+    finish_batch(S, take, resps, t_done);
   }
 }
 
